@@ -1,0 +1,516 @@
+// Host side of libsfac.so: the reference's C interface (sfac.hpp:194-211)
+// implemented over the sm_100a kernels.  Handle state, argument checks and
+// the state machine follow sfac.cpp; every computation on grids or atoms runs
+// on the GPU.  No C++ exception crosses the C ABI: failures return NULL/0 and
+// are recorded in the handle (sfac_last_error).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/sfac.h"
+#include "spme_kernels.hpp"
+
+using namespace spme;
+
+namespace {
+
+struct Handle {
+  int order = 0, K[3] = {0, 0, 0}, ldim = 0;
+  long nreal = 0, nmodes = 0, ncell = 0;
+  Geom geom{};
+  Spline spline{};
+  SplineNodes nodes{};
+  int state = -1;  // -1: nothing computed, 0: structure factor, 1: potential grid
+  int a_mode = 0;  // 0: no influence function, 1: host tables, 2: Ewald on device
+  Influence inf{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr;
+  // device buffers
+  float *d_real = nullptr;
+  float2 *d_cplx = nullptr;
+  double *d_iB[3] = {nullptr, nullptr, nullptr};
+  float2 *d_tw[3] = {nullptr, nullptr, nullptr};
+  FftPlan3 fft{};
+  double *d_A = nullptr;  // 7 * nmodes (table mode)
+  double *d_partials = nullptr, *d_red = nullptr;
+  int cap = 0;
+  double *d_x = nullptr, *d_w = nullptr;
+  SortBuffers sb{};
+  int gcap = 0;
+  double *d_gx = nullptr, *d_gw = nullptr, *d_gout = nullptr;
+  int last_n = 0;
+  // pinned host buffers
+  double *h_S = nullptr;
+  float *h_f = nullptr;
+  double *h_red = nullptr;
+  int err = 0;
+  char errstr[256] = {0};
+  long long launches = 0;
+};
+
+Handle *H(void *p) { return reinterpret_cast<Handle *>(p); }
+
+bool check(Handle *h, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  if (h) {
+    h->err = (int)e;
+    snprintf(h->errstr, sizeof(h->errstr), "%s: %s", what, cudaGetErrorString(e));
+    fprintf(stderr, "sfac: CUDA error in %s: %s\n", what, cudaGetErrorString(e));
+  }
+  return false;
+}
+#define CK(h, call) check((h), (call), #call)
+
+bool launched(Handle *h, int n, const char *what) {
+  h->launches += n;
+  return check(h, cudaGetLastError(), what);
+}
+
+template <class T>
+bool dalloc(Handle *h, T **p, size_t count) {
+  *p = nullptr;
+  return CK(h, cudaMalloc((void **)p, sizeof(T) * (count ? count : 1)));
+}
+template <class T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Cell(L): lower-triangular box, its inverse and 1/V, with the reference's
+// expressions and operation order (sfac.hpp:37-52) so that the keys computed
+// from these constants round exactly like the CPU's.
+void set_cell(Geom &g, const double L[6]) {
+  g.iV = 1. / (L[0] * L[1] * L[2]);
+  g.iL00 = 1. / L[0];
+  g.iL11 = 1. / L[1];
+  g.iL22 = 1. / L[2];
+  g.iL10 = -L[3] * L[2] * g.iV;
+  g.iL20 = (L[3] * L[5] - L[1] * L[4]) * g.iV;
+  g.iL21 = -L[0] * L[5] * g.iV;
+}
+
+// Coefficients of the cardinal B-spline pieces: row j, column i holds the
+// coefficient of t^(n-1-i) of M_n(t+j),
+//   C(n-1,i)/(n-1)! * sum_{k=0..j} (-1)^k C(n,k) (j-k)^i
+// (the explicit piecewise form that BSpline::mk_bspl_coeffs tabulates,
+// sfac.hpp:81-109).  Evaluated in long double, stored FP32 for the kernels
+// and as FP64 node values M_n(j) for the moduli.
+void make_spline(int n, Spline &S, SplineNodes &nodes) {
+  long double binom[kMaxOrder + 1][kMaxOrder + 1] = {};
+  for (int a = 0; a <= kMaxOrder; a++) {
+    binom[a][0] = 1;
+    for (int b = 1; b <= a; b++) binom[a][b] = binom[a - 1][b - 1] + (b <= a - 1 ? binom[a - 1][b] : 0);
+  }
+  long double fact = 1;
+  for (int k = 2; k < n; k++) fact *= k;
+  memset(&S, 0, sizeof(S));
+  memset(&nodes, 0, sizeof(nodes));
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) {
+      long double acc = 0;
+      for (int k = 0; k <= j; k++) {
+        long double pw = 1;
+        for (int e = 0; e < i; e++) pw *= (long double)(j - k);
+        acc += ((k & 1) ? -1 : 1) * binom[n][k] * pw;
+      }
+      const long double c = binom[n - 1][i] / fact * acc;
+      S.c[j * n + i] = (float)c;
+      if (i == n - 1) nodes.Mj[j] = (double)c;  // constant term: M_n(j)
+    }
+}
+
+void free_atoms(Handle *h) {
+  dfree(h->d_x);
+  dfree(h->d_w);
+  for (int i = 0; i < 2; i++) {
+    dfree(h->sb.keys[i]);
+    dfree(h->sb.vals[i]);
+  }
+  dfree(h->sb.rec);
+  dfree(h->sb.rec_sorted);
+  dfree(h->sb.hist);
+  h->cap = 0;
+}
+
+bool ensure_atoms(Handle *h, int n) {
+  if (n <= h->cap) return true;
+  free_atoms(h);
+  const int cap = n + n / 2 + 64;
+  bool ok = dalloc(h, &h->d_x, 3 * (size_t)cap) && dalloc(h, &h->d_w, cap);
+  for (int i = 0; i < 2; i++) ok = ok && dalloc(h, &h->sb.keys[i], cap) && dalloc(h, &h->sb.vals[i], cap);
+  ok = ok && dalloc(h, &h->sb.rec, cap) && dalloc(h, &h->sb.rec_sorted, cap) &&
+       dalloc(h, &h->sb.hist, sort_scratch_words(cap));
+  if (!ok) {
+    free_atoms(h);
+    return false;
+  }
+  h->cap = cap;
+  return true;
+}
+
+bool ensure_gather(Handle *h, int n) {
+  if (n <= h->gcap) return true;
+  dfree(h->d_gx);
+  dfree(h->d_gw);
+  dfree(h->d_gout);
+  const int cap = n + n / 2 + 64;
+  if (!(dalloc(h, &h->d_gx, 3 * (size_t)cap) && dalloc(h, &h->d_gw, cap) &&
+        dalloc(h, &h->d_gout, 3 * (size_t)cap))) {
+    h->gcap = 0;
+    return false;
+  }
+  h->gcap = cap;
+  return true;
+}
+
+void destroy(Handle *h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  dfree(h->d_real);
+  dfree(h->d_cplx);
+  for (int d = 0; d < 3; d++) {
+    dfree(h->d_iB[d]);
+    dfree(h->d_tw[d]);
+  }
+  dfree(h->d_A);
+  dfree(h->d_partials);
+  dfree(h->d_red);
+  dfree(h->sb.cell_start);
+  free_atoms(h);
+  dfree(h->d_gx);
+  dfree(h->d_gw);
+  dfree(h->d_gout);
+  if (h->h_S) cudaFreeHost(h->h_S);
+  if (h->h_f) cudaFreeHost(h->h_f);
+  if (h->h_red) cudaFreeHost(h->h_red);
+  if (h->ev_in) cudaEventDestroy(h->ev_in);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+bool sync(Handle *h) { return CK(h, cudaStreamSynchronize(h->stream)); }
+
+}  // namespace
+
+extern "C" {
+
+void *sfac_ctor(double L[6], int K[3], int order) {
+  if (order % 2 != 0 || order < 2 || order > kMaxOrder) {
+    printf("Bad order: %d (must be even)\n", order);
+    return nullptr;
+  }
+  if (K[0] < 1 || K[1] < 1 || K[2] < 1) {
+    printf("Bad K: %d %d %d\n", K[0], K[1], K[2]);
+    return nullptr;
+  }
+  const long ncell = (long)K[0] * K[1] * K[2];
+  if (ncell >= 0x7fffffffL) {
+    printf("Bad K: %d %d %d (grid too large)\n", K[0], K[1], K[2]);
+    return nullptr;
+  }
+  int dev = 0, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1 || cudaGetDevice(&dev) != cudaSuccess) {
+    printf("sfac_ctor: no CUDA device available\n");
+    cudaGetLastError();
+    return nullptr;
+  }
+  Handle *h = new (std::nothrow) Handle;
+  if (!h) return nullptr;
+  h->device = dev;
+  h->order = order;
+  for (int d = 0; d < 3; d++) h->K[d] = K[d];
+  h->ldim = K[2] / 2 + 1;
+  h->ncell = ncell;
+  h->nreal = ncell;
+  h->nmodes = (long)K[0] * K[1] * h->ldim;
+  Geom &g = h->geom;
+  g.K0 = K[0];
+  g.K1 = K[1];
+  g.K2 = K[2];
+  g.ldim = h->ldim;
+  g.order = order;
+  set_cell(g, L);
+  make_spline(order, h->spline, h->nodes);
+
+  bool ok = CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) &&
+            CK(h, cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+  ok = ok && dalloc(h, &h->d_real, h->nreal) && dalloc(h, &h->d_cplx, h->nmodes) &&
+       dalloc(h, &h->d_partials, (size_t)kConvBlocks * kRedWords) && dalloc(h, &h->d_red, kRedWords) &&
+       dalloc(h, &h->sb.cell_start, ncell + 1);
+  for (int d = 0; d < 3 && ok; d++) ok = dalloc(h, &h->d_iB[d], K[d]) && dalloc(h, &h->d_tw[d], K[d]);
+  const size_t hf = (size_t)(2 * h->nmodes > h->nreal ? 2 * h->nmodes : h->nreal);
+  ok = ok && CK(h, cudaMallocHost((void **)&h->h_S, sizeof(double) * 2 * h->nmodes)) &&
+       CK(h, cudaMallocHost((void **)&h->h_f, sizeof(float) * hf)) &&
+       CK(h, cudaMallocHost((void **)&h->h_red, sizeof(double) * kRedWords));
+  if (ok) {
+    memset(h->h_S, 0, sizeof(double) * 2 * h->nmodes);
+    int n = 0;
+    for (int d = 0; d < 3; d++) {
+      n += fft_make_len(h->fft.len[d], K[d], h->d_tw[d], h->stream);
+      n += launch_bspline_moduli(K[d], order, h->nodes, h->d_iB[d], h->stream);
+    }
+    ok = launched(h, n, "ctor kernels") && CK(h, cudaMemsetAsync(h->d_real, 0, sizeof(float) * h->nreal, h->stream)) &&
+         CK(h, cudaMemsetAsync(h->d_cplx, 0, sizeof(float2) * h->nmodes, h->stream)) && sync(h);
+  }
+  if (!ok) {
+    destroy(h);
+    cudaGetLastError();
+    return nullptr;
+  }
+  return h;
+}
+
+void sfac_dtor(void *p) { destroy(H(p)); }
+
+void sfac(void *p, int n, const double *w, const double *x) {
+  Handle *h = H(p);
+  if (!h) return;
+  if (n < 0) {
+    printf("sfac: bad atom count %d\n", n);
+    return;
+  }
+  if (!ensure_atoms(h, n)) return;
+  if (n > 0) {
+    if (!CK(h, cudaMemcpyAsync(h->d_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream)) ||
+        !CK(h, cudaMemcpyAsync(h->d_w, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream)))
+      return;
+  }
+  CK(h, cudaEventRecord(h->ev_in, h->stream));
+  int k = launch_cell_sort(h->geom, n, h->d_x, h->d_w, h->sb, h->stream);
+  k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.rec_sorted, h->d_real, h->stream);
+  DeconvArgs dc{h->d_iB[0], h->d_iB[1], h->d_iB[2], h->ldim};
+  k += launch_fft_forward(h->fft, h->d_real, h->d_cplx, dc, h->stream);
+  if (!launched(h, k, "sfac kernels")) return;
+  // The caller may reuse w and x once this returns: wait for the copies only.
+  CK(h, cudaEventSynchronize(h->ev_in));
+  h->last_n = n;
+  h->state = 0;
+}
+
+double *get_S(void *p) {
+  Handle *h = H(p);
+  if (!h) return nullptr;
+  if (h->state == 0) {
+    if (CK(h, cudaMemcpyAsync(h->h_f, h->d_cplx, sizeof(float2) * h->nmodes, cudaMemcpyDeviceToHost,
+                              h->stream)) &&
+        sync(h)) {
+      for (long i = 0; i < 2 * h->nmodes; i++) h->h_S[i] = (double)h->h_f[i];
+    }
+  } else if (h->state == 1) {
+    if (CK(h, cudaMemcpyAsync(h->h_f, h->d_real, sizeof(float) * h->nreal, cudaMemcpyDeviceToHost, h->stream)) &&
+        sync(h)) {
+      const long rows = (long)h->K[0] * h->K[1];
+      const int K2 = h->K[2], pitch = 2 * h->ldim;
+      for (long r = 0; r < rows; r++) {
+        double *dst = h->h_S + r * pitch;
+        const float *src = h->h_f + r * K2;
+        for (int k = 0; k < K2; k++) dst[k] = (double)src[k];
+        for (int k = K2; k < pitch; k++) dst[k] = 0.0;
+      }
+    }
+  }
+  return h->h_S;
+}
+
+void set_L(void *p, double L[6]) {
+  Handle *h = H(p);
+  if (!h) return;
+  set_cell(h->geom, L);
+}
+
+// Tabulates A and dA exactly as set_A defines them (sfac.cpp:213-292): every
+// lattice vector n with |m| < max_m, m = iL n, is folded onto its stored
+// half-space mode (the conjugate partner when n_z mod K2 >= ldim), adding
+// f(m^2)/2 to A and f'(m^2) m_a m_b to dA.  f runs on the host (it may be a
+// Python callable); the tables are then uploaded as FP64.
+int set_A(void *p, rad_fn f, double max_m, void *info) {
+  Handle *h = H(p);
+  if (!h) return 2;
+  const int K0 = h->K[0], K1 = h->K[1], K2 = h->K[2], ldim = h->ldim;
+  const long nm = h->nmodes;
+  std::vector<double> tab;
+  try {
+    tab.assign(7 * (size_t)nm, 0.0);
+  } catch (...) {
+    return 2;
+  }
+  double *A = tab.data(), *dA = A + nm;
+  const Geom &g = h->geom;
+  const double R2 = max_m * max_m;
+  const int i0 = (int)(max_m / g.iL00);
+  for (int i = -i0; i <= i0; i++) {
+    const double mx = i * g.iL00;
+    const double m20 = mx * mx;
+    const double dy = std::sqrt(std::fmax(R2 - m20, 0.0));
+    const double my0 = i * g.iL10;
+    const int j0 = (int)std::ceil((-dy - my0) / g.iL11);
+    const int j1 = (int)std::floor((dy - my0) / g.iL11);
+    for (int j = j0; j <= j1; j++) {
+      const double my = my0 + j * g.iL11;
+      const double m21 = m20 + my * my;
+      const double dz = std::sqrt(std::fmax(R2 - m21, 0.0));
+      const double mz0 = i * g.iL20 + j * g.iL21;
+      const int k0 = (int)std::ceil((-dz - mz0) / g.iL22);
+      const int k1 = (int)std::floor((dz - mz0) / g.iL22);
+      for (int k = k0; k <= k1; k++) {
+        const double mz = mz0 + k * g.iL22;
+        const double m2 = m21 + mz * mz;
+        const int kz = imod(k, K2);
+        long mode;
+        if (kz < ldim) mode = ((long)imod(i, K0) * K1 + imod(j, K1)) * ldim + kz;
+        else mode = ((long)imod(-i, K0) * K1 + imod(-j, K1)) * ldim + (K2 - kz);
+        double s = 0.0;
+        A[mode] += 0.5 * f(m2, &s, info);
+        double *d = dA + 6 * mode;
+        d[0] += s * mx * mx;
+        d[1] += s * my * my;
+        d[2] += s * mz * mz;
+        d[3] += s * my * mx;
+        d[4] += s * mz * mx;
+        d[5] += s * mz * my;
+      }
+    }
+  }
+  if (!h->d_A && !dalloc(h, &h->d_A, 7 * (size_t)nm)) return 2;
+  if (!CK(h, cudaMemcpyAsync(h->d_A, A, sizeof(double) * 7 * nm, cudaMemcpyHostToDevice, h->stream)) || !sync(h))
+    return 2;
+  h->inf = Influence{};
+  h->inf.mode = 1;
+  h->inf.A = h->d_A;
+  h->inf.dA = h->d_A + nm;
+  h->a_mode = 1;
+  return 0;
+}
+
+double en(void *p) {
+  Handle *h = H(p);
+  if (!h) return 0.0;
+  if (h->state != 0) {
+    printf("Error: You must call sfac before this routine.\n");
+    return 0.0;
+  }
+  if (h->a_mode == 0) {
+    printf("Error: No convolution kernel has been set.\n");
+    return 0.0;
+  }
+  int k = launch_conv(h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, 0, h->d_partials, h->d_red,
+                      h->stream);
+  if (!launched(h, k, "en kernels")) return 0.0;
+  if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
+      !sync(h))
+    return 0.0;
+  return h->h_red[0] * h->geom.iV;
+}
+
+double de1(void *p, double vir[6]) {
+  Handle *h = H(p);
+  if (!h) return 0.0;
+  if (h->state != 0) {
+    printf("Error: You must call sfac before this routine.\n");
+    return 0.0;
+  }
+  if (h->a_mode == 0) {
+    printf("Error: No convolution kernel has been set.\n");
+    return 0.0;
+  }
+  int k = launch_conv(h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, 1, h->d_partials, h->d_red,
+                      h->stream);
+  k += launch_fft_inverse(h->fft, h->d_cplx, h->d_real, h->stream);
+  if (!launched(h, k, "de1 kernels")) return 0.0;
+  if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
+      !sync(h))
+    return 0.0;
+  const double *r = h->h_red;
+  const double fac = h->geom.iV * h->geom.iV;
+  vir[0] = (r[1] + r[0]) * fac;
+  vir[1] = (r[2] + r[0]) * fac;
+  vir[2] = (r[3] + r[0]) * fac;
+  vir[3] = r[4] * fac;
+  vir[4] = r[5] * fac;
+  vir[5] = r[6] * fac;
+  h->state = 1;
+  return r[0] * h->geom.iV;
+}
+
+static void gather_call(Handle *h, int n, const double *w, const double *x, double *dx, double *phi) {
+  if (h->state != 1) {
+    printf("Error: You must call de1 before this routine.\n");
+    return;
+  }
+  if (n <= 0) return;
+  if (!ensure_gather(h, n)) return;
+  if (!CK(h, cudaMemcpyAsync(h->d_gx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream))) return;
+  if (w && !CK(h, cudaMemcpyAsync(h->d_gw, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream))) return;
+  int k = launch_gather(h->geom, h->spline, n, h->d_gx, h->d_gw, h->d_real, dx ? h->d_gout : nullptr,
+                        phi ? h->d_gout : nullptr, h->stream);
+  if (!launched(h, k, "gather kernel")) return;
+  if (dx)
+    CK(h, cudaMemcpyAsync(dx, h->d_gout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
+  else
+    CK(h, cudaMemcpyAsync(phi, h->d_gout, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  sync(h);
+}
+
+void de2(void *p, int n, const double *w, const double *x, double *dx) {
+  Handle *h = H(p);
+  if (!h) return;
+  gather_call(h, n, w, x, dx, nullptr);
+}
+
+void potl(void *p, int n, const double *x, double *phi) {
+  Handle *h = H(p);
+  if (!h) return;
+  gather_call(h, n, nullptr, x, nullptr, phi);
+}
+
+int sfac_set_ewald(void *p, double beta, double max_m) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (!(beta > 0.0) || !(max_m >= 0.0)) {
+    printf("sfac_set_ewald: bad beta %g or max_m %g\n", beta, max_m);
+    return 1;
+  }
+  Influence &inf = h->inf;
+  inf = Influence{};
+  inf.mode = 2;
+  inf.iL00 = h->geom.iL00;
+  inf.iL10 = h->geom.iL10;
+  inf.iL11 = h->geom.iL11;
+  inf.iL20 = h->geom.iL20;
+  inf.iL21 = h->geom.iL21;
+  inf.iL22 = h->geom.iL22;
+  inf.beta = beta;
+  inf.max_m = max_m;
+  h->a_mode = 2;
+  return 0;
+}
+
+int sfac_last_error(void *p) { return p ? H(p)->err : -1; }
+const char *sfac_error_string(void *p) { return p ? H(p)->errstr : "null handle"; }
+int sfac_device(void *p) { return p ? H(p)->device : -1; }
+long long sfac_kernel_launches(void *p) { return p ? H(p)->launches : 0; }
+
+int sfac_debug_sort(void *p, int n, int *keys, int *perm) {
+  Handle *h = H(p);
+  if (!h || n != h->last_n || h->state < 0) return 1;
+  if (n == 0) return 0;
+  if (!CK(h, cudaMemcpyAsync(keys, h->sb.keys[h->sb.cur], sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream)) ||
+      !CK(h, cudaMemcpyAsync(perm, h->sb.vals[h->sb.cur], sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream)))
+    return 1;
+  return sync(h) ? 0 : 1;
+}
+
+int sfac_debug_spread(void *p, float *grid) {
+  Handle *h = H(p);
+  if (!h || h->state != 0) return 1;
+  if (!CK(h, cudaMemcpyAsync(grid, h->d_real, sizeof(float) * h->nreal, cudaMemcpyDeviceToHost, h->stream)))
+    return 1;
+  return sync(h) ? 0 : 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+// Shared definitions for the SPME reciprocal-space kernels (sm_100a).
+//
+// Grid conventions follow the reference (sfac.hpp:160-192):
+//   real grid      [K0][K1][K2]      (x-major, z contiguous; unpadded here)
+//   complex grid   [K0][K1][ldim]    ldim = K2/2 + 1 (half-complex last axis)
+// Fractional coordinates s = iL^T x (Cell::scale, sfac.hpp:56-62) with the
+// lower-triangular inverse box iL of Cell (sfac.hpp:37-52).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace spme {
+
+constexpr int kMaxOrder = 8;  // MAX_SPL_ORDER (sfac.hpp:7); enforced here
+
+// Box and grid constants, passed by value to every kernel.
+struct Geom {
+  int K0, K1, K2, ldim, order;
+  // iL lower triangle (Cell::iL) and 1/V, FP64 (host-computed, sfac.hpp:45-51)
+  double iL00, iL10, iL11, iL20, iL21, iL22, iV;
+};
+
+// order x order polynomial table of the cardinal B-spline M_n: row j holds
+// the Horner coefficients of M_n(t + j), t in [0,1) (BSpline, sfac.hpp:81-109).
+struct Spline {
+  float c[kMaxOrder * kMaxOrder];
+};
+
+__host__ __device__ inline int imod(int a, int b) { return ((a % b) + b) % b; }
+
+// M_n(t + j) by Horner (BSpline::bspl_coef, sfac.hpp:124-131), FP32.
+__device__ __forceinline__ float bspl_eval(const Spline &S, int n, float t, int j) {
+  const float *r = S.c + j * n;
+  float b = r[0];
+#pragma unroll 8
+  for (int i = 1; i < kMaxOrder; i++)
+    if (i < n) b = fmaf(b, t, r[i]);
+  return b;
+}
+
+// Value and derivative (BSpline::dbspl_coef, sfac.hpp:146-157), FP32.
+__device__ __forceinline__ void dbspl_eval(const Spline &S, int n, float t, int j,
+                                           float &b, float &db) {
+  const float *r = S.c + j * n;
+  float d = r[0];
+  float v = fmaf(r[0], t, r[1]);
+#pragma unroll 8
+  for (int i = 2; i < kMaxOrder; i++)
+    if (i < n) {
+      d = fmaf(d, t, v);
+      v = fmaf(v, t, r[i]);
+    }
+  b = v;
+  db = d;
+}
+
+// Fractional coordinate component, rounded exactly as Cell::scale computes
+// it on the host: ((x0*a + x1*b) + x2*c), no FMA contraction, then wrap.
+__device__ __forceinline__ double wrap01_rn(double v) { return __dsub_rn(v, floor(v)); }
+
+__device__ __forceinline__ void frac_coords(const Geom &g, double x0, double x1, double x2,
+                                            double &s0, double &s1, double &s2) {
+  s0 = wrap01_rn(__dadd_rn(__dadd_rn(__dmul_rn(x0, g.iL00), __dmul_rn(x1, g.iL10)),
+                           __dmul_rn(x2, g.iL20)));
+  s1 = wrap01_rn(__dadd_rn(__dmul_rn(x1, g.iL11), __dmul_rn(x2, g.iL21)));
+  s2 = wrap01_rn(__dmul_rn(x2, g.iL22));
+}
+
+}  // namespace spme

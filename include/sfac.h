@@ -1,0 +1,107 @@
+/*
+ * sfac.h -- C ABI of libsfac.so, the B200 (sm_100a) SPME reciprocal-space
+ * library.
+ *
+ * The first block is a drop-in for the C interface of the reference
+ * (frobnitzem/EwaldCorrel, sfac.hpp:194-211): same symbol names, argument
+ * meanings, array layouts, state machine and error behaviour, so the
+ * reference's ctypes wrapper (ewald.py:15-68) binds it unchanged.  All
+ * arrays are HOST memory, FP64, C-contiguous.  Each handle owns its device
+ * buffers and a CUDA stream on the device that was current at sfac_ctor.
+ *
+ * The second block adds entry points the reference does not have; they never
+ * change the behaviour of the first block.
+ */
+#ifndef SFAC_B200_H
+#define SFAC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- reference interface (sfac.hpp:194-211) ---------------- */
+
+/* rad_fn must return f(r2) and store f'(r2) in *dA; info is passed through
+ * (sfac.hpp:201-203). */
+typedef double (*rad_fn)(double r2, double *dA, void *info);
+
+/* Replaces sfac_ctor (sfac.hpp:196, sfac.cpp:180-183).
+ * L = [ax, by, cz, bx, cx, cy] (lower-triangular box rows), K = grid size,
+ * order = even B-spline order in [2, 8].  Returns NULL (never throws) on an
+ * odd or out-of-range order, K < 1, a grid too large for 32-bit cell keys,
+ * no CUDA device, or an allocation failure. */
+void *sfac_ctor(double L[6], int K[3], int order);
+
+/* Replaces sfac_dtor (sfac.hpp:197, sfac.cpp:185-188).  Releases only this
+ * handle (the reference's global fftw_cleanup has no counterpart). */
+void sfac_dtor(void *sfac);
+
+/* Replaces sfac (sfac.hpp:198, sfac.cpp:190-193): spread the n weights w
+ * at positions x (n x 3), forward FFT, divide by the B-spline moduli.
+ * State becomes 0 (structure factor). */
+void sfac(void *sfac, int n, const double *w, const double *x);
+
+/* Replaces get_S (sfac.hpp:199, sfac.cpp:194-197).  Returns a host array
+ * owned by the handle, valid until sfac_dtor: in state 0 the structure
+ * factor as K0 x K1 x ldim x 2 doubles (ldim = K2/2+1); in state 1 the real
+ * potential grid as K0 x K1 x (2*ldim) doubles (first K2 of each row used).
+ * The array is refreshed from the device at each call. */
+double *get_S(void *sfac);
+
+/* Replaces set_L (sfac.hpp:205, sfac.cpp:199-202): replaces the box only;
+ * the influence function is NOT recomputed. */
+void set_L(void *sfac, double L[6]);
+
+/* Replaces set_A (sfac.hpp:206, sfac.cpp:213-292): tabulates A = sum f/2 and
+ * dA = sum f' m_a m_b over every m = iL n with |m| < max_m, folded onto the
+ * stored half space, calling f on the host.  Returns 0, or 2 on an
+ * allocation failure. */
+int set_A(void *sfac, rad_fn f, double max_m, void *info);
+
+/* Replaces en (sfac.hpp:207, sfac.cpp:304-325): iV * sum A |S|^2.
+ * Needs state 0 and an influence function, else prints and returns 0. */
+double en(void *sfac);
+
+/* Replaces de1 (sfac.hpp:208, sfac.cpp:339-396): energy, virial
+ * vir = [xx, yy, zz, yx, zx, zy], convolution and inverse FFT into the
+ * potential grid.  Needs state 0; state becomes 1. */
+double de1(void *sfac, double vir[6]);
+
+/* Replaces de2 (sfac.hpp:209, sfac.cpp:409-483): dE/dx (n x 3) of weights
+ * w at positions x (any point set).  Needs state 1. */
+void de2(void *sfac, int n, const double *w, const double *x, double *dx);
+
+/* Replaces potl (sfac.hpp:210, sfac.cpp:497-545): potential phi (n) at
+ * positions x.  Needs state 1. */
+void potl(void *sfac, int n, const double *x, double *phi);
+
+/* ---------------- additions (no counterpart in the reference) ----------- */
+
+/* Ewald influence function f(m^2) = exp(-pi^2 m^2/beta^2)/(pi m^2) with the
+ * same image set as set_A(ewald_f, max_m) (ewald.py:124-132), evaluated in
+ * FP64 on the device at each use instead of tabulated on the host.  Uses the
+ * cell current at this call (later set_L calls do not change it, as with
+ * set_A).  Returns 0. */
+int sfac_set_ewald(void *sfac, double beta, double max_m);
+
+/* Last CUDA or argument error seen by this handle (0 = none), and its text. */
+int sfac_last_error(void *sfac);
+const char *sfac_error_string(void *sfac);
+
+/* Device the handle runs on, and the number of kernels it has launched. */
+int sfac_device(void *sfac);
+long long sfac_kernel_launches(void *sfac);
+
+/* Debug views (copies to host; for parity tests).
+ * sfac_debug_sort: cell keys and original indices in sorted order (n each)
+ *   of the last sfac call.
+ * sfac_debug_spread: the spread grid of the last sfac call (K0*K1*K2 float),
+ *   recomputed from the stored sorted atoms. */
+int sfac_debug_sort(void *sfac, int n, int *keys, int *perm);
+int sfac_debug_spread(void *sfac, float *grid);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SFAC_B200_H */
