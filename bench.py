@@ -1,0 +1,449 @@
+"""SPME reciprocal-space benchmark on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: the water box (98,304 atoms = 32,768 rigid 3-site molecules in a
+10 nm cube, 96^3 grid, B-spline order 4, Ewald beta 3.12 nm^-1), seeded
+synthetic data.  One step = one full reciprocal solve: cell sort, spread,
+forward FFT, convolution with energy and virial, inverse FFT, and the gather
+of forces (dE/dx) and potentials at every atom.
+
+Metric: solves/s (whole job; replicas on N GPUs -- the path does not shard).
+``value`` is timed with CUDA events on the launching stream with inputs
+resident in HBM and the L2 flushed (256 MiB write) before every step; ``e2e``
+is the same metric through the reference-compatible C API (sfac, de1, de2,
+potl) with pinned host buffers, host<->device copies inside the timed
+region.  The CPU baseline is the reference's own sfac.cpp (oracle/_ref,
+compiled -O3 -fopenmp) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "water": ("water box: 98,304 atoms (32,768 rigid 3-site molecules), 10 nm cube, 96^3 grid, "
+              "B-spline order 4, Ewald beta 3.12 nm^-1",
+              "SPME solves/s (water box 98,304 atoms, 96^3, order 4)"),
+    "triclinic": ("triclinic cell: 1,048,576 charges N(0, 0.5^2), a=b=c=20 nm, gamma=60 deg, 256^3 grid, "
+                  "B-spline order 6, Ewald beta 3.5 nm^-1",
+                  "SPME solves/s (1,048,576 charges, 256^3, order 6, triclinic)"),
+}
+WORKLOAD, METRIC = WORKLOADS["water"]
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            # wait (bounded) for the first sample so the timed region is covered
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [t.strip() for t in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------- algorithmic bytes --
+def algorithmic_bytes(n, K):
+    """Algorithmic HBM bytes per stage of one solve (FP64 atom I/O, FP32
+    grids): inputs read once by the spread and once by the gather, outputs
+    written once; spread writes the real grid G, R2C reads G and writes the
+    half-complex grid H, the convolution reads and writes H, C2R reads H and
+    writes G, the gather reads G."""
+    K0, K1, K2 = K
+    G = 4 * K0 * K1 * K2
+    H = 8 * K0 * K1 * (K2 // 2 + 1)
+    atom_in = n * (3 * 8 + 8)
+    atom_out = n * (3 * 8 + 8)
+    return {
+        "cell_sort": atom_in,
+        "spread": G,
+        "fft_forward": G + H,
+        "convolution": 2 * H,
+        "fft_inverse": H + G,
+        "gather": G + atom_in + atom_out,
+        "solve_total": 2 * atom_in + atom_out + 4 * G + 2 * H,
+    }
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# -------------------------------------------------------- CPU sides --
+def _load_reference_solver():
+    """The reference's sfac.cpp compiled unmodified (oracle/_ref), else the
+    oracle's C restatement.  Used only for the CPU baseline and the
+    reference arm."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle import oracle as O
+
+    if O.ref_available():
+        return O.RefSfac, "reference", "reference sfac.cpp (oracle/_ref, g++ -O3 -fopenmp, FFT: project FP64 shim; FFTW unavailable)"
+    return O.OracleSfac, "port", "oracle C restatement (oracle/liborc.so, gcc -O3 -fopenmp)"
+
+
+def cpu_setup(cls, c):
+    """Handle + influence function (setup: outside the timed solves)."""
+    s = cls(c.L, np.array(c.K), c.order)
+    s.set_ewald(c.beta, c.max_m)
+    return s
+
+
+def cpu_solve(s, c):
+    s.sfac(c.q, c.x)
+    vir = np.zeros(6)
+    e = s.de1(vir)
+    dx = np.zeros((c.n, 3))
+    phi = np.zeros(c.n)
+    s.de2(c.n, c.q, c.x, dx)
+    s.potl(c.n, c.x, phi)
+    return e, vir, dx, phi
+
+
+def cpu_baseline(c, budget_s=20.0, max_solves=10):
+    cls, kind, desc = _load_reference_solver()
+    s = cpu_setup(cls, c)
+    t0 = time.perf_counter()
+    res = cpu_solve(s, c)
+    t1 = time.perf_counter()
+    times = [t1 - t0]
+    while sum(times) < budget_s * 0.5 and len(times) < max_solves:
+        a = time.perf_counter()
+        cpu_solve(s, c)
+        times.append(time.perf_counter() - a)
+    s.close()
+    per = statistics.median(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {
+        "value": 1.0 / per, "unit": "solves/s", "cores": cores, "kind": kind,
+        "sample": f"{len(times)} full water-box solves (sfac+de1+de2+potl, setup excluded), median {per * 1e3:.1f} ms; {desc}",
+    }, res
+
+
+# ------------------------------------------------------------- GPU arm --
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    from ewaldcorrel_b200 import configs
+    from ewaldcorrel_b200 import ewald as ew
+    from ewaldcorrel_b200.device import STAGES, SpmeSolver
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    c = configs.cfg2_water() if args.workload == "water" else configs.cfg3_triclinic()
+    WORKLOAD, METRIC = WORKLOADS[args.workload]
+    n = c.n
+    stream = torch.cuda.Stream(dev)
+    solver = SpmeSolver(c.L, c.K, c.order, c.beta, c.max_m, device=local_rank, stream=stream)
+    with torch.cuda.stream(stream):
+        x = torch.from_numpy(c.x).to(dev)
+        q = torch.from_numpy(c.q).to(dev)
+        dx = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        phi = torch.empty(n, dtype=torch.float64, device=dev)
+        ev = torch.empty(7, dtype=torch.float64, device=dev)
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # clocks are sampled from before the warm-up until after the e2e timing
+    clk = ClockSampler(local_rank).__enter__()
+
+    # warm-up
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            flush.zero_()
+            solver.solve(x, q, dx, phi, ev)
+    barrier()
+
+    # timed region: K solves, each bracketed by events, L2 flushed between
+    K = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    l0 = solver.launches()
+    barrier()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            starts[k].record(stream)
+            solver.solve(x, q, dx, phi, ev)
+            ends[k].record(stream)
+    barrier()
+    launches = solver.launches() - l0
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    total_ms_max = float(tmax.item())
+    value = world * K / (total_ms_max / 1e3)
+    srt = sorted(step_ms)
+    p50 = srt[len(srt) // 2]
+    p99 = srt[min(len(srt) - 1, int(math.ceil(0.99 * len(srt))) - 1)]
+    ev_host = ev.cpu().numpy()
+
+    # per-stage times (same solve with events between stages), L2 flushed
+    stage_acc = {s: [] for s in STAGES}
+    for _ in range(max(3, min(K, 10))):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        st = solver.solve_timed(x, q, dx, phi, ev)
+        for s_, v in st.items():
+            stage_acc[s_].append(v)
+    stage_ms = {s_: statistics.mean(v) for s_, v in stage_acc.items()}
+    alg = algorithmic_bytes(n, c.K)
+    dominant = max(STAGES, key=lambda s_: stage_ms[s_])
+    peak, peak_kind = measured_peak()
+    achieved = alg[dominant] / (stage_ms[dominant] / 1e3) / 1e9
+
+    # end to end through the reference-compatible C API, pinned host buffers
+    xh = torch.from_numpy(c.x).pin_memory().numpy()
+    qh = torch.from_numpy(c.q).pin_memory().numpy()
+    dxh = torch.zeros((n, 3), dtype=torch.float64).pin_memory().numpy()
+    phih = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
+    sf = ew.Sfac(c.L, np.array(c.K), c.order)
+    sf.set_ewald(c.beta, c.max_m)
+    vir = np.zeros(6)
+    for _ in range(3):
+        sf.sfac(qh, xh)
+        sf.de1(vir)
+        sf.de2(n, qh, xh, dxh)
+        sf.potl(n, xh, phih)
+    e2e_ms = []
+    for _ in range(K):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        a = time.perf_counter()
+        sf.sfac(qh, xh)
+        e_api = sf.de1(vir)
+        sf.de2(n, qh, xh, dxh)
+        sf.potl(n, xh, phih)
+        e2e_ms.append((time.perf_counter() - a) * 1e3)
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * K / (float(e2e_t.item()) / 1e3)
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms_max / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (grids, FFT, spline weights); f64 (positions, cell keys, moduli, influence function, energy/virial reductions)",
+        "data": f"synthetic (seeded numpy rng({2 if args.workload == 'water' else 3}); no dataset)",
+        "config": {
+            "workload": WORKLOAD,
+            "atoms": n,
+            "grid": list(c.K),
+            "order": c.order,
+            "beta": c.beta,
+            "max_m": c.max_m,
+            "parallelism": f"replicas x{world} (independent solves, no collective)",
+            "l2": "flushed before every timed step (256 MiB device write, outside the step events)",
+        },
+        "latency_ms": {"p50": p50, "p99": p99, "mean": total_ms_max / K},
+        "stage_ms": stage_ms,
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dominant,
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
+            "algorithmic_bytes": alg[dominant],
+            "solve_algorithmic_bytes": alg["solve_total"],
+            "solve_frac": alg["solve_total"] / (total_ms_max / K / 1e3) / 1e9 / peak,
+        },
+        "e2e": {
+            "value": e2e_value,
+            "unit": "solves/s",
+            "h2d_bytes_per_step": int(n * (24 + 8) * 2 + n * 24),
+            "d2h_bytes_per_step": int(n * 24 + n * 8 + 7 * 8),
+            "api": "sfac + de1 + de2 + potl (reference C interface), pinned host arrays",
+        },
+        "gpu_launches": int(launches),
+        "energy": float(ev_host[0]),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, (e_ref, vir_ref, dx_ref, phi_ref) = cpu_baseline(c)
+        line["cpu_baseline"] = cb
+        dxg = dx.cpu().numpy()
+        phig = phi.cpu().numpy()
+        line["accuracy_vs_reference"] = {
+            "energy_rel_err": abs(float(ev_host[0]) - e_ref) / abs(e_ref),
+            "force_rel_rms": float(np.sqrt(np.mean((dxg - dx_ref) ** 2) / np.mean(dx_ref ** 2))),
+            "potential_rel_rms": float(np.sqrt(np.mean((phig - phi_ref) ** 2) / np.mean(phi_ref ** 2))),
+            "virial_max_rel": float(np.abs(ev_host[1:] - vir_ref).max() / np.abs(vir_ref).max()),
+        }
+    line["clocks"] = clocks
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------ reference arm --
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from ewaldcorrel_b200 import configs
+
+    try:
+        cls, kind, desc = _load_reference_solver()
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"CPU reference not built: {e}"}))
+        return
+    c = configs.cfg2_water()
+    s = cpu_setup(cls, c)
+    for _ in range(max(0, args.warmup)):
+        cpu_solve(s, c)
+    times = []
+    for _ in range(args.steps):
+        a = time.perf_counter()
+        cpu_solve(s, c)
+        times.append(time.perf_counter() - a)
+    s.close()
+    total = sum(times)
+    value = args.steps / total
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    srt = sorted(times)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded numpy rng(2); no dataset)",
+        "config": {"workload": WORKLOAD, "atoms": c.n, "grid": list(c.K), "order": c.order, "beta": c.beta,
+                   "max_m": c.max_m, "parallelism": "CPU, OpenMP threads"},
+        "latency_ms": {"p50": srt[len(srt) // 2] * 1e3, "p99": srt[-1] * 1e3},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind,
+                         "sample": f"{args.steps} full water-box solves (sfac+de1+de2+potl, setup excluded); {desc}"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS))
+    args = ap.parse_args(argv)
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+// Influence function of the reciprocal convolution, per stored mode
+// (set_A, sfac.cpp:213-292; ewald.py:124-132), FP64, and FP64 reductions.
+#pragma once
+
+#include "spme_kernels.hpp"
+
+namespace spme {
+
+// Ewald influence function f(m^2) = exp(-pi^2 m^2 / beta^2) / (pi m^2) and
+// f'(m^2) = (-pi^2/beta^2 - 1/m^2) f  (ewald.py:124-132; f(0) = 0).
+__device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
+  if (r2 < 1e-10) {
+    fp = 0.0;
+    return 0.0;
+  }
+  const double f = exp(r2 * fac) / (r2 * 3.14159265358979323846);
+  fp = (fac - 1.0 / r2) * f;
+  return f;
+}
+
+// Sum of f and f' m_a m_b over the reciprocal vectors m = iL (i,j,k) with
+// |m| < max_m whose lattice index is congruent to the stored mode
+// (kx, ky, kz) -- the images set_A visits and folds onto this mode
+// (sfac.cpp:240-289, same sphere bounds, FP64 without contraction).  The
+// conjugate images that set_A folds onto interior modes have the same f
+// values, so the caller doubles those instead of revisiting them.
+__device__ __forceinline__ void ewald_images(const Influence &inf, int K0, int K1, int K2, int kx, int ky, int kz,
+                             double &sf, double sd[6]) {
+  const double R2 = __dmul_rn(inf.max_m, inf.max_m);
+  const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
+  const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
+  sf = 0.0;
+  for (int c = 0; c < 6; c++) sd[c] = 0.0;
+  for (int i = -i0 + imod(kx + i0, K0); i <= i0; i += K0) {
+    const double mx = __dmul_rn((double)i, inf.iL00);
+    const double m20 = __dmul_rn(mx, mx);
+    const double dy = sqrt(fmax(__dsub_rn(R2, m20), 0.0));
+    const double my0 = __dmul_rn((double)i, inf.iL10);
+    const int j0 = (int)ceil(__ddiv_rn(__dsub_rn(-dy, my0), inf.iL11));
+    const int j1 = (int)floor(__ddiv_rn(__dsub_rn(dy, my0), inf.iL11));
+    for (int j = j0 + imod(ky - j0, K1); j <= j1; j += K1) {
+      const double my = __dadd_rn(my0, __dmul_rn((double)j, inf.iL11));
+      const double m21 = __dadd_rn(m20, __dmul_rn(my, my));
+      const double dz = sqrt(fmax(__dsub_rn(R2, m21), 0.0));
+      const double mz0 = __dadd_rn(__dmul_rn((double)i, inf.iL20), __dmul_rn((double)j, inf.iL21));
+      const int k0 = (int)ceil(__ddiv_rn(__dsub_rn(-dz, mz0), inf.iL22));
+      const int k1 = (int)floor(__ddiv_rn(__dsub_rn(dz, mz0), inf.iL22));
+      for (int k = k0 + imod(kz - k0, K2); k <= k1; k += K2) {
+        const double mz = __dadd_rn(mz0, __dmul_rn((double)k, inf.iL22));
+        const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
+        double fp;
+        sf += ewald_f(m2, fac, fp);
+        sd[0] += fp * mx * mx;
+        sd[1] += fp * my * my;
+        sd[2] += fp * mz * mz;
+        sd[3] += fp * my * mx;
+        sd[4] += fp * mz * mx;
+        sd[5] += fp * mz * my;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Image pairs (i, j) of row (kx, ky) and their z bounds, exactly as
+// ewald_images enumerates them.  Returns the pair count, or -1 when the row
+// has more than kRowPairs pairs.
+__device__ __forceinline__ int ewald_row(const Influence &inf, int K0, int K1, int kx, int ky, RowImg &r) {
+  const double R2 = __dmul_rn(inf.max_m, inf.max_m);
+  const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
+  int c = 0;
+  for (int i = -i0 + imod(kx + i0, K0); i <= i0; i += K0) {
+    const double mx = __dmul_rn((double)i, inf.iL00);
+    const double m20 = __dmul_rn(mx, mx);
+    const double dy = sqrt(fmax(__dsub_rn(R2, m20), 0.0));
+    const double my0 = __dmul_rn((double)i, inf.iL10);
+    const int j0 = (int)ceil(__ddiv_rn(__dsub_rn(-dy, my0), inf.iL11));
+    const int j1 = (int)floor(__ddiv_rn(__dsub_rn(dy, my0), inf.iL11));
+    for (int j = j0 + imod(ky - j0, K1); j <= j1; j += K1) {
+      if (c >= kRowPairs) return -1;
+      const double my = __dadd_rn(my0, __dmul_rn((double)j, inf.iL11));
+      const double m21 = __dadd_rn(m20, __dmul_rn(my, my));
+      const double dz = sqrt(fmax(__dsub_rn(R2, m21), 0.0));
+      const double mz0 = __dadd_rn(__dmul_rn((double)i, inf.iL20), __dmul_rn((double)j, inf.iL21));
+      r.k0[c] = (int)ceil(__ddiv_rn(__dsub_rn(-dz, mz0), inf.iL22));
+      r.k1[c] = (int)floor(__ddiv_rn(__dsub_rn(dz, mz0), inf.iL22));
+      r.mx[c] = mx;
+      r.my[c] = my;
+      r.m21[c] = m21;
+      r.mz0[c] = mz0;
+      c++;
+    }
+  }
+  return c;
+}
+
+// Same sums as ewald_images from a row's precomputed pairs: per pair only
+// the z images (k = kz mod K2 within [k0, k1]) and their exp are evaluated.
+__device__ __forceinline__ void ewald_images_row(const Influence &inf, const RowImg &r, int K2, int kz, double &sf,
+                                                 double sd[6]) {
+  const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
+  sf = 0.0;
+  for (int c = 0; c < 6; c++) sd[c] = 0.0;
+  const int n = r.count;
+  for (int c = 0; c < n; c++) {
+    const int k0 = r.k0[c], k1 = r.k1[c];
+    const double mx = r.mx[c], my = r.my[c], m21 = r.m21[c], mz0 = r.mz0[c];
+    // first k >= k0 with k = kz (mod K2)
+    const int d = kz - k0;
+    int k = k0 + (d >= 0 ? d - (int)inf.K2d.div((uint32_t)d) * K2
+                         : (K2 - 1) - (int)((uint32_t)(-d - 1) - inf.K2d.div((uint32_t)(-d - 1)) * K2));
+    for (; k <= k1; k += K2) {
+      const double mz = __dadd_rn(mz0, __dmul_rn((double)k, inf.iL22));
+      const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
+      double fp;
+      sf += ewald_f(m2, fac, fp);
+      sd[0] += fp * mx * mx;
+      sd[1] += fp * my * my;
+      sd[2] += fp * mz * mz;
+      sd[3] += fp * my * mx;
+      sd[4] += fp * mz * mx;
+      sd[5] += fp * mz * my;
+    }
+  }
+}
+
+// A (with set_A's half weight on the kz = 0 and even-K2 Nyquist planes) and
+// dA (6 components) of stored mode (kx, ky, kz), index i = (kx*K1 + ky)*ldim + kz.
+__device__ __forceinline__ void mode_influence(const Influence &inf, const Geom &g, long i, int kx, int ky,
+                                               int kz, bool plane, double &A, double dA[6]) {
+  if (inf.mode == 1) {
+    A = inf.A[i];
+#pragma unroll
+    for (int c = 0; c < 6; c++) dA[c] = inf.dA[6 * i + c];
+  } else {
+    double sf, sd[6];
+    const RowImg &r = inf.rows[(long)kx * g.K1 + ky];
+    if (r.count >= 0) ewald_images_row(inf, r, g.K2, kz, sf, sd);
+    else ewald_images(inf, g.K0, g.K1, g.K2, kx, ky, kz, sf, sd);
+    // set_A adds f/2 from each image and from each conjugate image
+    // (interior modes), and f' m m in full from both.
+    const double wA = plane ? 0.5 : 1.0;
+    A = wA * sf;
+#pragma unroll
+    for (int c = 0; c < 6; c++) dA[c] = 2.0 * wA * sd[c];
+  }
+}
+
+// Deterministic reduction of 7 FP64 per-thread sums over a block: fixed
+// shuffle tree per warp, then warps in order.  Thread c < 7 of warp 0 ends
+// with the block total of component c in out[c] (shared, 8 x 7 doubles).
+__device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*red)[7], double *out_global) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 7; c++) {
+    const double v = warp_sum(acc[c]);
+    if (lane == 0) red[warp][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
+    out_global[threadIdx.x] = v;
+  }
+}
+
+// Sum of the block partials (warp c sums component c: lanes take blocks in
+// a fixed stride, then a fixed shuffle tree), and the final energy/virial
+// ev = [E, vir_xx, vir_yy, vir_zz, vir_yx, vir_zx, vir_zy] as de1 forms them
+// (sfac.cpp:384-395).  Needs >= 7 warps; raw receives the 7 sums.
+__device__ __forceinline__ void finish_partials(const double *__restrict__ partials, int nblocks, double iV,
+                                                double *__restrict__ raw, double *__restrict__ ev) {
+  __shared__ double tot[7];
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c < 7) {
+    double v = 0.0;
+    for (int b = lane; b < nblocks; b += 32) v += partials[(long)b * kRedWords + c];
+    v = warp_sum(v);
+    if (lane == 0) {
+      tot[c] = v;
+      if (raw) raw[c] = v;
+    }
+  }
+  __syncthreads();
+  if (ev && threadIdx.x == 0) {
+    const double fac = iV * iV;
+    ev[0] = tot[0] * iV;
+    ev[1] = (tot[1] + tot[0]) * fac;
+    ev[2] = (tot[2] + tot[0]) * fac;
+    ev[3] = (tot[3] + tot[0]) * fac;
+    ev[4] = tot[4] * fac;
+    ev[5] = tot[5] * fac;
+    ev[6] = tot[6] * fac;
+  }
+}
+
+}  // namespace spme

@@ -7,7 +7,7 @@
 // a fixed grid of kConvBlocks blocks walks the modes with a fixed stride,
 // each block reduces with a fixed shuffle tree, and one final block sums the
 // block partials in index order.  No atomics.
-#include "spme_kernels.hpp"
+#include "influence.cuh"
 
 namespace spme {
 
@@ -27,68 +27,7 @@ int launch_bspline_moduli(int n, int order, const SplineNodes &nodes, double *iB
   return 1;
 }
 
-// Ewald influence function f(m^2) = exp(-pi^2 m^2 / beta^2) / (pi m^2) and
-// f'(m^2) = (-pi^2/beta^2 - 1/m^2) f  (ewald.py:124-132; f(0) = 0).
-__device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
-  if (r2 < 1e-10) {
-    fp = 0.0;
-    return 0.0;
-  }
-  const double f = exp(r2 * fac) / (r2 * 3.14159265358979323846);
-  fp = (fac - 1.0 / r2) * f;
-  return f;
-}
-
-// Sum of f and f' m_a m_b over the reciprocal vectors m = iL (i,j,k) with
-// |m| < max_m whose lattice index is congruent to the stored mode
-// (kx, ky, kz) -- the images set_A visits and folds onto this mode
-// (sfac.cpp:240-289, same sphere bounds, FP64 without contraction).  The
-// conjugate images that set_A folds onto interior modes have the same f
-// values, so the caller doubles those instead of revisiting them.
-__device__ void ewald_images(const Influence &inf, int K0, int K1, int K2, int kx, int ky, int kz,
-                             double &sf, double sd[6]) {
-  const double R2 = __dmul_rn(inf.max_m, inf.max_m);
-  const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
-  const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
-  sf = 0.0;
-  for (int c = 0; c < 6; c++) sd[c] = 0.0;
-  for (int i = -i0 + imod(kx + i0, K0); i <= i0; i += K0) {
-    const double mx = __dmul_rn((double)i, inf.iL00);
-    const double m20 = __dmul_rn(mx, mx);
-    const double dy = sqrt(fmax(__dsub_rn(R2, m20), 0.0));
-    const double my0 = __dmul_rn((double)i, inf.iL10);
-    const int j0 = (int)ceil(__ddiv_rn(__dsub_rn(-dy, my0), inf.iL11));
-    const int j1 = (int)floor(__ddiv_rn(__dsub_rn(dy, my0), inf.iL11));
-    for (int j = j0 + imod(ky - j0, K1); j <= j1; j += K1) {
-      const double my = __dadd_rn(my0, __dmul_rn((double)j, inf.iL11));
-      const double m21 = __dadd_rn(m20, __dmul_rn(my, my));
-      const double dz = sqrt(fmax(__dsub_rn(R2, m21), 0.0));
-      const double mz0 = __dadd_rn(__dmul_rn((double)i, inf.iL20), __dmul_rn((double)j, inf.iL21));
-      const int k0 = (int)ceil(__ddiv_rn(__dsub_rn(-dz, mz0), inf.iL22));
-      const int k1 = (int)floor(__ddiv_rn(__dsub_rn(dz, mz0), inf.iL22));
-      for (int k = k0 + imod(kz - k0, K2); k <= k1; k += K2) {
-        const double mz = __dadd_rn(mz0, __dmul_rn((double)k, inf.iL22));
-        const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
-        double fp;
-        sf += ewald_f(m2, fac, fp);
-        sd[0] += fp * mx * mx;
-        sd[1] += fp * my * my;
-        sd[2] += fp * mz * mz;
-        sd[3] += fp * my * mx;
-        sd[4] += fp * mz * mx;
-        sd[5] += fp * mz * my;
-      }
-    }
-  }
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-template <int MODE, bool SCALE>
+template <bool SCALE>
 __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const double *__restrict__ iB0,
                                                    const double *__restrict__ iB1,
                                                    const double *__restrict__ iB2, float2 *__restrict__ S,
@@ -107,20 +46,7 @@ __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const 
     const double s = (double)q.x * q.x + (double)q.y * q.y;
     const bool plane = (kz == 0) || (even && kz == ldim - 1);
     double A, dA[6];
-    if (MODE == 1) {
-      A = inf.A[i];
-#pragma unroll
-      for (int c = 0; c < 6; c++) dA[c] = inf.dA[6 * i + c];
-    } else {
-      double sf, sd[6];
-      ewald_images(inf, g.K0, K1, g.K2, kx, ky, kz, sf, sd);
-      // set_A adds f/2 from each image and from each conjugate image
-      // (interior modes), and f' m m in full from both.
-      const double wA = plane ? 0.5 : 1.0;
-      A = wA * sf;
-#pragma unroll
-      for (int c = 0; c < 6; c++) dA[c] = 2.0 * wA * sd[c];
-    }
+    mode_influence(inf, g, i, kx, ky, kz, plane, A, dA);
     acc[0] += s * A;
 #pragma unroll
     for (int c = 0; c < 6; c++) acc[1 + c] += s * dA[c];
@@ -131,43 +57,44 @@ __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const 
     }
   }
   __shared__ double red[8][7];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < 7; c++) {
-    const double v = warp_sum(acc[c]);
-    if (lane == 0) red[warp][c] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 7) {
-    double v = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
-    partials[(long)blockIdx.x * kRedWords + threadIdx.x] = v;
-  }
+  block_reduce7(acc, red, partials + (long)blockIdx.x * kRedWords);
 }
 
-__global__ void conv_finish_kernel(const double *__restrict__ partials, int nblocks, double *__restrict__ out) {
-  const int c = threadIdx.x;
-  if (c >= 7) return;
-  double v = 0.0;
-  for (int b = 0; b < nblocks; b++) v += partials[(long)b * kRedWords + c];
-  out[c] = v;
+__global__ void conv_finish_kernel(const double *__restrict__ partials, int nblocks, double iV,
+                                   double *__restrict__ raw, double *__restrict__ ev) {
+  finish_partials(partials, nblocks, iV, raw, ev);
 }
 
 int launch_conv(const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
-                 const double *iB2, float2 *S, int want_scale, double *partials, double *out,
-                 cudaStream_t st) {
+                const double *iB2, float2 *S, int want_scale, double *partials, double *out, double *ev,
+                cudaStream_t st) {
   const long nm = (long)g.K0 * g.K1 * g.ldim;
   int blocks = (int)((nm + 255) / 256);
   if (blocks > kConvBlocks) blocks = kConvBlocks;
-  if (inf.mode == 1) {
-    if (want_scale) conv_kernel<1, true><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
-    else conv_kernel<1, false><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
-  } else {
-    if (want_scale) conv_kernel<2, true><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
-    else conv_kernel<2, false><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
-  }
-  conv_finish_kernel<<<1, 32, 0, st>>>(partials, blocks, out);
+  if (want_scale) conv_kernel<true><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
+  else conv_kernel<false><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
+  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, blocks, g.iV, out, ev);
   return 2;
+}
+
+__global__ void ewald_rows_kernel(Geom g, Influence inf, RowImg *rows) {
+  const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= (long)g.K0 * g.K1) return;
+  RowImg row;
+  row.count = ewald_row(inf, g.K0, g.K1, (int)(r / g.K1), (int)(r % g.K1), row);
+  row.pad = 0;
+  rows[r] = row;
+}
+
+int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStream_t st) {
+  const long n = (long)g.K0 * g.K1;
+  ewald_rows_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, inf, rows);
+  return 1;
+}
+
+int launch_finish(const double *partials, int nblocks, double iV, double *raw, double *ev, cudaStream_t st) {
+  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, nblocks, iV, raw, ev);
+  return 1;
 }
 
 }  // namespace spme

@@ -10,178 +10,16 @@
 // 7 butterflies written out and a direct-DFT butterfly for any other prime,
 // and stores the lines back.  Twiddles come from an FP32 table built in FP64
 // (fft_twiddle_kernel).
-#include "spme_kernels.hpp"
+#include "fft_engine.cuh"
+#include "influence.cuh"
 
 namespace spme {
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-// sign * i * a
-template <int SIGN>
-__device__ __forceinline__ float2 rot(float2 a) {
-  return SIGN < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
-}
-template <int SIGN>
-__device__ __forceinline__ float2 twid(const float2 *tw, int k) {
-  float2 w = tw[k];
-  if (SIGN > 0) w.y = -w.y;
-  return w;
-}
-
-// In-register R-point DFTs, X[q] = sum_r v[r] exp(SIGN 2 pi i r q / R).
-template <int R, int SIGN>
-struct Bfly;
-
-template <int SIGN>
-struct Bfly<2, SIGN> {
-  __device__ static void run(float2 *v, const float2 *, int) {
-    float2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
-  }
-};
-template <int SIGN>
-struct Bfly<3, SIGN> {
-  __device__ static void run(float2 *v, const float2 *, int) {
-    const float c = -0.5f, s = 0.86602540378443864676f;
-    float2 t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    float2 mid = make_float2(fmaf(c, t.x, v[0].x), fmaf(c, t.y, v[0].y));
-    float2 r = rot<SIGN>(cscale(d, s));
-    v[0] = cadd(v[0], t);
-    v[1] = cadd(mid, r);
-    v[2] = csub(mid, r);
-  }
-};
-template <int SIGN>
-struct Bfly<4, SIGN> {
-  __device__ static void run(float2 *v, const float2 *, int) {
-    float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    float2 t2 = cadd(v[1], v[3]), t3 = rot<SIGN>(csub(v[1], v[3]));
-    v[0] = cadd(t0, t2);
-    v[2] = csub(t0, t2);
-    v[1] = cadd(t1, t3);
-    v[3] = csub(t1, t3);
-  }
-};
-template <int SIGN>
-struct Bfly<5, SIGN> {
-  __device__ static void run(float2 *v, const float2 *, int) {
-    const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
-    const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
-    float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-    float2 m1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
-    float2 m2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
-    float2 r1 = rot<SIGN>(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
-    float2 r2 = rot<SIGN>(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
-    v[0] = cadd(v[0], cadd(t1, t2));
-    v[1] = cadd(m1, r1);
-    v[4] = csub(m1, r1);
-    v[2] = cadd(m2, r2);
-    v[3] = csub(m2, r2);
-  }
-};
-// Any other radix: direct DFT with roots from the length-n table
-// (w_R = tw[n/R]).
-template <int R, int SIGN>
-struct Bfly {
-  __device__ static void run(float2 *v, const float2 *tw, int n) {
-    float2 out[R];
-    const int step = n / R;
-#pragma unroll
-    for (int q = 0; q < R; q++) {
-      float2 acc = v[0];
-#pragma unroll
-      for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid<SIGN>(tw, ((r * q) % R) * step)));
-      out[q] = acc;
-    }
-#pragma unroll
-    for (int q = 0; q < R; q++) v[q] = out[q];
-  }
-};
-
-// One Stockham stage over B lines: in/out are [j][b] with pitch P.
-template <int R, int SIGN>
-__device__ __forceinline__ void stage(const float2 *in, float2 *out, const float2 *tw, int n, int Ns,
-                                      int B, int P) {
-  const int m = n / R;
-  const int twstep = n / (Ns * R);
-  for (int item = threadIdx.x; item < m * B; item += blockDim.x) {
-    const int b = item % B, j = item / B;
-    const int k = j % Ns;
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      v[r] = in[(j + r * m) * P + b];
-      if (r > 0) v[r] = cmul(v[r], twid<SIGN>(tw, r * k * twstep));
-    }
-    Bfly<R, SIGN>::run(v, tw, n);
-    const int idxD = (j / Ns) * Ns * R + k;
-#pragma unroll
-    for (int r = 0; r < R; r++) out[(idxD + r * Ns) * P + b] = v[r];
-  }
-}
-
-// Radices outside the compiled set: the same stage, reading the inputs
-// straight from shared memory (O(R^2) per butterfly, any R).
-template <int SIGN>
-__device__ void stage_any(const float2 *in, float2 *out, const float2 *tw, int n, int R, int Ns, int B,
-                          int P) {
-  const int m = n / R;
-  const int twstep = n / (Ns * R);
-  const int step = n / R;
-  for (int item = threadIdx.x; item < m * B * R; item += blockDim.x) {
-    const int q = item % R;
-    const int rest = item / R;
-    const int b = rest % B, j = rest / B;
-    const int k = j % Ns;
-    float2 acc = make_float2(0.f, 0.f);
-    for (int r = 0; r < R; r++) {
-      float2 x = in[(j + r * m) * P + b];
-      x = cmul(x, twid<SIGN>(tw, r * k * twstep));
-      acc = cadd(acc, cmul(x, twid<SIGN>(tw, ((r * q) % R) * step)));
-    }
-    const int idxD = (j / Ns) * Ns * R + k;
-    out[(idxD + q * Ns) * P + b] = acc;
-  }
-}
-
-// Runs all stages; returns the buffer holding the result.
-template <int SIGN>
-__device__ float2 *run_stages(const FftLen &L, float2 *b0, float2 *b1, const float2 *tw, int B, int P) {
-  int Ns = 1;
-  for (int s = 0; s < L.nst; s++) {
-    const int R = L.rad[s];
-    switch (R) {
-      case 2: stage<2, SIGN>(b0, b1, tw, L.n, Ns, B, P); break;
-      case 3: stage<3, SIGN>(b0, b1, tw, L.n, Ns, B, P); break;
-      case 4: stage<4, SIGN>(b0, b1, tw, L.n, Ns, B, P); break;
-      case 5: stage<5, SIGN>(b0, b1, tw, L.n, Ns, B, P); break;
-      case 7: stage<7, SIGN>(b0, b1, tw, L.n, Ns, B, P); break;
-      default: stage_any<SIGN>(b0, b1, tw, L.n, R, Ns, B, P); break;
-    }
-    __syncthreads();
-    float2 *t = b0;
-    b0 = b1;
-    b1 = t;
-    Ns *= R;
-  }
-  return b0;
-}
-
-__device__ __forceinline__ void load_twiddles(float2 *tw_s, const FftLen &L) {
-  for (int i = threadIdx.x; i < L.n; i += blockDim.x) tw_s[i] = L.tw[i];
-}
 
 // --- z pass, forward: real rows -> half-complex rows --------------------
 // CTA handles 2B real rows (B complex lines); row pitch K2 (real) / ldim.
 __global__ void __launch_bounds__(256) fft_z_r2c_kernel(FftLen L, int nrows, const float *__restrict__ rin,
                                                         float2 *__restrict__ cout, int ldim, int B,
-                                                        int bufsz) {
+                                                        int bufsz, FastDiv Bd) {
   extern __shared__ float2 sm[];
   const int n = L.n, P = B + 1;
   float2 *tw = sm, *b0 = sm + n, *b1 = b0 + bufsz;
@@ -195,7 +33,7 @@ __global__ void __launch_bounds__(256) fft_z_r2c_kernel(FftLen L, int nrows, con
     slot[rl & 1] = v;
   }
   __syncthreads();
-  float2 *res = run_stages<-1>(L, b0, b1, tw, B, P);
+  float2 *res = run_stages<-1>(L, b0, b1, tw, Bd, P);
   for (int e = threadIdx.x; e < 2 * B * ldim; e += blockDim.x) {
     const int rl = e / ldim, k = e % ldim;
     const long row = row0 + rl;
@@ -214,7 +52,7 @@ __global__ void __launch_bounds__(256) fft_z_r2c_kernel(FftLen L, int nrows, con
 // real part only, as a c2r transform does.
 __global__ void __launch_bounds__(256) fft_z_c2r_kernel(FftLen L, int nrows, const float2 *__restrict__ cin,
                                                         float *__restrict__ rout, int ldim, int B,
-                                                        int bufsz) {
+                                                        int bufsz, FastDiv Bd) {
   extern __shared__ float2 sm[];
   const int n = L.n, P = B + 1;
   float2 *tw = sm, *b0 = sm + n, *b1 = b0 + bufsz;
@@ -242,7 +80,7 @@ __global__ void __launch_bounds__(256) fft_z_c2r_kernel(FftLen L, int nrows, con
     b0[k * P + b] = z;
   }
   __syncthreads();
-  float2 *res = run_stages<+1>(L, b0, b1, tw, B, P);
+  float2 *res = run_stages<+1>(L, b0, b1, tw, Bd, P);
   for (int e = threadIdx.x; e < 2 * B * n; e += blockDim.x) {
     const int rl = e / n, z = e % n;
     const long row = row0 + rl;
@@ -260,7 +98,7 @@ __global__ void __launch_bounds__(256) fft_z_c2r_kernel(FftLen L, int nrows, con
 template <int SIGN>
 __global__ void __launch_bounds__(256) fft_strided_kernel(FftLen L, long nlines, long inner, long outer,
                                                           long stride, float2 *__restrict__ data, int B,
-                                                          int bufsz, DeconvArgs dc) {
+                                                          int bufsz, DeconvArgs dc, FastDiv Bd) {
   extern __shared__ float2 sm[];
   const int n = L.n, P = B + 1;
   float2 *tw = sm, *b0 = sm + n, *b1 = b0 + bufsz;
@@ -274,7 +112,7 @@ __global__ void __launch_bounds__(256) fft_strided_kernel(FftLen L, long nlines,
     b0[j * P + b] = v;
   }
   __syncthreads();
-  float2 *res = run_stages<SIGN>(L, b0, b1, tw, B, P);
+  float2 *res = run_stages<SIGN>(L, b0, b1, tw, Bd, P);
   for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
     const int b = e % B, j = e / B;
     const long line = line0 + b;
@@ -287,6 +125,171 @@ __global__ void __launch_bounds__(256) fft_strided_kernel(FftLen L, long nlines,
       v = cscale(v, t);
     }
     data[(line / inner) * outer + (line % inner) + j * stride] = v;
+  }
+}
+
+
+// --- fused plane pass, forward: one CTA per x-plane -----------------------
+// z r2c of the plane's K1 real rows (two rows per complex line), then the
+// y transform of its ldim columns, both in shared memory; one read of the
+// real plane, one write of the half-complex plane.
+__global__ void __launch_bounds__(512) fft_plane_fwd_kernel(FftLen Ly, FftLen Lz, const float *__restrict__ rin,
+                                                            float2 *__restrict__ cout, int sz, FastDiv d_nb1,
+                                                            FastDiv d_ldim) {
+  extern __shared__ float2 sm[];
+  const int K1 = Ly.n, K2 = Lz.n, ldim = K2 / 2 + 1;
+  float2 *twy = sm, *twz = twy + K1, *A = twz + K2, *Bf = A + sz;
+  load_twiddles(twy, Ly);
+  load_twiddles(twz, Lz);
+  const long x = blockIdx.x;
+  const float *plane = rin + x * K1 * K2;
+  float2 *out = cout + x * K1 * ldim;
+  const int nb1 = (K1 + 1) / 2, P1 = nb1 + 1, P2 = ldim + 1;
+  for (int e = threadIdx.x; e < K1 * K2; e += blockDim.x) {
+    const int y = e / K2, z = e % K2;
+    reinterpret_cast<float *>(&A[z * P1 + (y >> 1)])[y & 1] = plane[e];
+  }
+  if (K1 & 1)
+    for (int z = threadIdx.x; z < K2; z += blockDim.x) A[z * P1 + nb1 - 1].y = 0.f;
+  __syncthreads();
+  float2 *R1 = run_stages<-1>(Lz, A, Bf, twz, d_nb1, P1);
+  float2 *O = (R1 == A) ? Bf : A;
+  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) {
+    const int y = e / ldim, k = e % ldim, b = y >> 1;
+    const float2 u = R1[k * P1 + b], v = R1[((K2 - k) % K2) * P1 + b];
+    O[y * P2 + k] = (y & 1) ? make_float2(0.5f * (u.y + v.y), -0.5f * (u.x - v.x))
+                            : make_float2(0.5f * (u.x + v.x), 0.5f * (u.y - v.y));
+  }
+  __syncthreads();
+  float2 *R2 = run_stages<-1>(Ly, O, R1, twy, d_ldim, P2);
+  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) out[e] = R2[(e / ldim) * P2 + e % ldim];
+}
+
+// --- fused plane pass, inverse: y transform then z c2r per x-plane -------
+// CTA 0 first reduces the energy/virial partials of the preceding x pass
+// (when `partials` is given): the reduction needs no extra launch.
+__global__ void __launch_bounds__(512) fft_plane_inv_kernel(FftLen Ly, FftLen Lz, const float2 *__restrict__ cin,
+                                                            float *__restrict__ rout, int sz,
+                                                            const double *__restrict__ partials, int nblocks,
+                                                            double iV, double *__restrict__ raw,
+                                                            double *__restrict__ ev, FastDiv d_nb1,
+                                                            FastDiv d_ldim) {
+  if (partials && blockIdx.x == 0) finish_partials(partials, nblocks, iV, raw, ev);
+  extern __shared__ float2 sm[];
+  const int K1 = Ly.n, K2 = Lz.n, ldim = K2 / 2 + 1;
+  float2 *twy = sm, *twz = twy + K1, *A = twz + K2, *Bf = A + sz;
+  load_twiddles(twy, Ly);
+  load_twiddles(twz, Lz);
+  const long x = blockIdx.x;
+  const float2 *in = cin + x * K1 * ldim;
+  float *plane = rout + x * K1 * K2;
+  const int nb1 = (K1 + 1) / 2, P1 = nb1 + 1, P2 = ldim + 1;
+  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) A[(e / ldim) * P2 + e % ldim] = in[e];
+  __syncthreads();
+  float2 *R = run_stages<+1>(Ly, A, Bf, twy, d_ldim, P2);
+  float2 *O = (R == A) ? Bf : A;
+  // complex lines z = X_{2b} + i X_{2b+1} over the full K2 (Hermitian
+  // extension; self-conjugate bins contribute their real part only)
+  for (int e = threadIdx.x; e < K2 * nb1; e += blockDim.x) {
+    const int b = e % nb1, k = e / nb1;
+    const int kk = (k < ldim) ? k : K2 - k;
+    const bool selfc = (kk == 0) || (2 * kk == K2);
+    float2 a = R[(2 * b) * P2 + kk];
+    float2 c = (2 * b + 1 < K1) ? R[(2 * b + 1) * P2 + kk] : make_float2(0.f, 0.f);
+    if (selfc) {
+      a.y = 0.f;
+      c.y = 0.f;
+    }
+    O[k * P1 + b] = (k < ldim) ? make_float2(a.x - c.y, a.y + c.x) : make_float2(a.x + c.y, c.x - a.y);
+  }
+  __syncthreads();
+  float2 *R2 = run_stages<+1>(Lz, O, R, twz, d_nb1, P1);
+  for (int e = threadIdx.x; e < K1 * K2; e += blockDim.x) {
+    const int y = e / K2, z = e % K2;
+    const float2 v = R2[z * P1 + (y >> 1)];
+    plane[e] = (y & 1) ? v.y : v.x;
+  }
+}
+
+// --- x pass with the pointwise reciprocal step ---------------------------
+// Lines (ky, kz) of length K0 (stride K1*ldim), B per CTA.
+//   XM_FWD_DECONV : forward, then S = F iB0 iB1 iB2          (sfac, sfac.cpp:125-138)
+//   XM_CONV_INV   : S given; energy/virial sums of |S|^2, S *= A iB (x2 on the
+//                   kz = 0 / even-K2 Nyquist planes), inverse (de1, sfac.cpp:357-392)
+//   XM_FWD_CONV_INV: forward, then the same with S = F iB, inverse (fused solve)
+// Energy/virial sums are FP64, reduced per CTA in a fixed order into
+// partials[blockIdx.x].
+//   XM_EN         : S given; the energy/virial sums only (en, sfac.cpp:304-325),
+//                   with exactly XM_CONV_INV's blocks and per-thread order, so
+//                   en() and de1() return the same energy bit for bit.
+enum { XM_FWD_DECONV = 0, XM_CONV_INV = 1, XM_FWD_CONV_INV = 2, XM_EN = 3 };
+
+template <int MODE>
+__global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence inf, const double *__restrict__ iB0,
+                                                    const double *__restrict__ iB1, const double *__restrict__ iB2,
+                                                    float2 *__restrict__ data, int B, int bufsz,
+                                                    double *__restrict__ partials, FastDiv Bd) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[8][7];
+  const int n = L.n, P = B + 1, ldim = g.ldim, K1 = g.K1;
+  const long nlines = (long)K1 * ldim;
+  float2 *tw = sm, *b0 = sm + n, *b1 = b0 + bufsz;
+  load_twiddles(tw, L);
+  const long line0 = (long)blockIdx.x * B;
+  for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
+    const int b = e % B, j = e / B;
+    const long line = line0 + b;
+    b0[j * P + b] = (line < nlines) ? data[line + j * nlines] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2 *cur = b0;
+  if (MODE == XM_FWD_DECONV || MODE == XM_FWD_CONV_INV) cur = run_stages<-1>(L, b0, b1, tw, Bd, P);
+  float2 *oth = (cur == b0) ? b1 : b0;
+  if (MODE == XM_FWD_DECONV) {
+    for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
+      const int b = e % B, j = e / B;
+      const long line = line0 + b;
+      if (line >= nlines) continue;
+      const int ky = (int)(line / ldim), kz = (int)(line % ldim);
+      cur[j * P + b] = cscale(cur[j * P + b], (float)(iB0[j] * iB1[ky] * iB2[kz]));
+    }
+    __syncthreads();
+  } else {
+    const bool even = (g.K2 % 2) == 0;
+    double acc[7];
+#pragma unroll
+    for (int c = 0; c < 7; c++) acc[c] = 0.0;
+    for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
+      const int b = e % B, j = e / B;
+      const long line = line0 + b;
+      if (line >= nlines) continue;
+      const int ky = (int)(line / ldim), kz = (int)(line % ldim), kx = j;
+      const long i = ((long)kx * K1 + ky) * ldim + kz;
+      const bool plane = (kz == 0) || (even && kz == ldim - 1);
+      const float2 q = cur[j * P + b];
+      const double ib = iB0[kx] * iB1[ky] * iB2[kz];
+      double s = (double)q.x * q.x + (double)q.y * q.y;
+      if (MODE == XM_FWD_CONV_INV) s *= ib * ib;  // |F iB|^2
+      double A, dA[6];
+      mode_influence(inf, g, i, kx, ky, kz, plane, A, dA);
+      acc[0] += s * A;
+#pragma unroll
+      for (int c = 0; c < 6; c++) acc[1 + c] += s * dA[c];
+      if (MODE != XM_EN) {
+        double t = A * ib * (MODE == XM_FWD_CONV_INV ? ib : 1.0);
+        if (plane) t *= 2.0;
+        cur[j * P + b] = cscale(q, (float)t);
+      }
+    }
+    block_reduce7(acc, red, partials + (long)blockIdx.x * kRedWords);
+    if (MODE == XM_EN) return;
+    __syncthreads();
+    cur = run_stages<+1>(L, cur, oth, tw, Bd, P);
+  }
+  for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
+    const int b = e % B, j = e / B;
+    const long line = line0 + b;
+    if (line < nlines) data[line + j * nlines] = cur[j * P + b];
   }
 }
 
@@ -309,73 +312,160 @@ int fft_make_len(FftLen &L, int n, float2 *tw_dev, cudaStream_t st) {
     while (m % p == 0) { L.rad[L.nst++] = p; m /= p; }
     if ((long)p * p > m && m > 1) { L.rad[L.nst++] = m; m = 1; }
   }
+  int Ns = 1;
+  for (int s = 0; s < L.nst; s++) {
+    L.ns[s] = FastDiv((uint32_t)Ns);
+    Ns *= L.rad[s];
+  }
   L.tw = tw_dev;
   fft_twiddle_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, tw_dev);
   return 1;
 }
 
-// Lines per CTA and shared-memory size for a pass over lines of length n.
-static void fft_shape(int n, int &B, int &bufsz, size_t &smem) {
+// Lines per CTA and shared-memory size for a pass over `nlines` lines of
+// length n: as many lines as fit 96 KB, then fewer while the pass would have
+// under four CTAs per SM (148 SMs), down to 4 lines (32-byte segments).
+static void fft_shape(int n, long nlines, int &B, int &bufsz, size_t &smem) {
   B = 64;
   while (B > 1 && (size_t)(n + 2 * (size_t)n * (B + 1)) * sizeof(float2) > 96 * 1024) B >>= 1;
+  while (B > 4 && (nlines + B - 1) / B < 4 * 148) B >>= 1;
   bufsz = n * (B + 1);
   const int need_c2r = 2 * B * (n / 2 + 1);
   if (need_c2r > bufsz) bufsz = need_c2r;
   smem = (size_t)(n + 2 * (size_t)bufsz) * sizeof(float2);
 }
 
-static void set_smem(const void *fn, size_t smem) {
-  if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+void fft_prepare_kernels() {
+  const int lim = 200 * 1024;
+  cudaFuncSetAttribute((const void *)fft_z_r2c_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_z_c2r_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_strided_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_strided_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_plane_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_plane_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x_kernel<XM_FWD_DECONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x_kernel<XM_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       lim);
+  cudaFuncSetAttribute((const void *)fft_x_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
-int launch_fft_forward(const FftPlan3 &F, const float *real, float2 *cplx, const DeconvArgs &dc,
+// Shared memory of the plane kernels: twiddles + two buffers of `sz`.
+static size_t plane_smem(int K1, int K2, int &sz) {
+  const int ldim = K2 / 2 + 1, nb1 = (K1 + 1) / 2;
+  sz = K2 * (nb1 + 1);
+  if (K1 * (ldim + 1) > sz) sz = K1 * (ldim + 1);
+  return (size_t)(K1 + K2 + 2 * (size_t)sz) * sizeof(float2);
+}
+constexpr size_t kPlaneSmemMax = 200 * 1024;
+
+bool fft_plane_fits(int K1, int K2) {
+  int sz;
+  return plane_smem(K1, K2, sz) <= kPlaneSmemMax;
+}
+
+long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 3) / 4; }
+
+// Forward z (r2c) and y transforms: one fused plane kernel when an x-plane
+// fits in shared memory, else one pass per axis.
+int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st) {
+  const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
+  int sz;
+  const size_t psm = plane_smem(K1, K2, sz);
+  if (psm <= kPlaneSmemMax) {
+    fft_plane_fwd_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], real, cplx, sz, FastDiv((K1 + 1) / 2),
+                                               FastDiv(ldim));
+    return 1;
+  }
+  int B, bufsz;
+  size_t smem;
+  const int nrows = K0 * K1;
+  fft_shape(K2, (nrows + 1) / 2, B, bufsz, smem);
+  fft_z_r2c_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, real, cplx, ldim, B, bufsz,
+                                                                      FastDiv(B));
+  const long nl = (long)K0 * ldim;
+  fft_shape(K1, nl, B, bufsz, smem);
+  DeconvArgs none{};
+  fft_strided_kernel<-1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim, ldim,
+                                                                     cplx, B, bufsz, none, FastDiv(B));
+  return 2;
+}
+
+// Inverse y and z (c2r) transforms; with `partials`, the energy/virial
+// partials are reduced first (inside the plane kernel when it is used).
+int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks, double iV,
+           double *raw, double *ev, cudaStream_t st) {
+  const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
+  int sz;
+  const size_t psm = plane_smem(K1, K2, sz);
+  if (psm <= kPlaneSmemMax) {
+    fft_plane_inv_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], cplx, real, sz, partials, nblocks, iV, raw, ev,
+                                               FastDiv((K1 + 1) / 2), FastDiv(ldim));
+    return 1;
+  }
+  int k = 0;
+  if (partials) k += launch_finish(partials, nblocks, iV, raw, ev, st);
+  int B, bufsz;
+  size_t smem;
+  const long nl = (long)K0 * ldim;
+  fft_shape(K1, nl, B, bufsz, smem);
+  DeconvArgs none{};
+  fft_strided_kernel<+1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim, ldim,
+                                                                     cplx, B, bufsz, none, FastDiv(B));
+  const int nrows = K0 * K1;
+  fft_shape(K2, (nrows + 1) / 2, B, bufsz, smem);
+  fft_z_c2r_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, cplx, real, ldim, B, bufsz,
+                                                                      FastDiv(B));
+  return k + 2;
+}
+
+template <int MODE>
+static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                  const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st) {
+  const long nl = (long)g.K1 * g.ldim;
+  int B, bufsz;
+  size_t smem;
+  fft_shape(g.K0, nl, B, bufsz, smem);
+  nblocks = (int)((nl + B - 1) / B);
+  fft_x_kernel<MODE><<<nblocks, 256, smem, st>>>(F.len[0], g, inf, iB0, iB1, iB2, cplx, B, bufsz, partials,
+                                                 FastDiv(B));
+  return 1;
+}
+
+int launch_fft_forward(const FftPlan3 &F, const Geom &g, const float *real, float2 *cplx, const DeconvArgs &dc,
                        cudaStream_t st) {
-  const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
-  int B, bufsz;
-  size_t smem;
-  // z: real rows -> half-complex rows
-  fft_shape(K2, B, bufsz, smem);
-  const int nrows = K0 * K1;
-  set_smem((const void *)fft_z_r2c_kernel, smem);
-  fft_z_r2c_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, real, cplx, ldim, B,
-                                                                      bufsz);
-  DeconvArgs none{};
-  // y: lines (x, kz), stride ldim
-  fft_shape(K1, B, bufsz, smem);
-  set_smem((const void *)fft_strided_kernel<-1>, smem);
-  long nl = (long)K0 * ldim;
-  fft_strided_kernel<-1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim,
-                                                                     ldim, cplx, B, bufsz, none);
-  // x: lines (y, kz), stride K1*ldim, with the moduli division
-  fft_shape(K0, B, bufsz, smem);
-  set_smem((const void *)fft_strided_kernel<-1>, smem);
-  nl = (long)K1 * ldim;
-  fft_strided_kernel<-1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[0], nl, nl, 0, nl, cplx, B,
-                                                                     bufsz, dc);
-  return 3;
+  int nb;
+  Influence none{};
+  return fwd_zy(F, real, cplx, st) + x_pass<XM_FWD_DECONV>(F, g, none, dc.iB0, dc.iB1, dc.iB2, cplx, nullptr, nb, st);
 }
 
-int launch_fft_inverse(const FftPlan3 &F, float2 *cplx, float *real, cudaStream_t st) {
-  const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
-  int B, bufsz;
-  size_t smem;
-  DeconvArgs none{};
-  fft_shape(K0, B, bufsz, smem);
-  set_smem((const void *)fft_strided_kernel<+1>, smem);
-  long nl = (long)K1 * ldim;
-  fft_strided_kernel<+1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[0], nl, nl, 0, nl, cplx, B,
-                                                                     bufsz, none);
-  fft_shape(K1, B, bufsz, smem);
-  set_smem((const void *)fft_strided_kernel<+1>, smem);
-  nl = (long)K0 * ldim;
-  fft_strided_kernel<+1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim,
-                                                                     ldim, cplx, B, bufsz, none);
-  fft_shape(K2, B, bufsz, smem);
-  const int nrows = K0 * K1;
-  set_smem((const void *)fft_z_c2r_kernel, smem);
-  fft_z_c2r_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, cplx, real, ldim, B,
-                                                                      bufsz);
-  return 3;
+int launch_conv_inverse(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
+                        const double *iB1, const double *iB2, float2 *cplx, float *real, double *partials,
+                        double *raw, double *ev, cudaStream_t st) {
+  int nb;
+  int k = x_pass<XM_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
+  return k + inv_yz(F, cplx, real, partials, nb, g.iV, raw, ev, st);
+}
+
+int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                  const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st) {
+  int nb;
+  x_pass<XM_EN>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
+  return 1 + launch_finish(partials, nb, g.iV, raw, nullptr, st);
+}
+
+int launch_x_conv(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                  const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st) {
+  return x_pass<XM_FWD_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nblocks, st);
+}
+
+int launch_fft_conv_solve(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
+                          const double *iB1, const double *iB2, const float *real_in, float2 *cplx,
+                          float *real_out, double *partials, double *raw, double *ev, cudaStream_t st) {
+  int nb;
+  int k = fwd_zy(F, real_in, cplx, st);
+  k += x_pass<XM_FWD_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
+  return k + inv_yz(F, cplx, real_out, partials, nb, g.iV, raw, ev, st);
 }
 
 }  // namespace spme

@@ -2,90 +2,122 @@
 //
 // The reference inserts every atom into a std::multimap keyed by
 // cid = (n0*K1 + n1)*K2 + n2; equal keys keep insertion order, so the result
-// is the STABLE sort of atoms by cid.  Here: one FP64 key kernel (rounding
-// identical to the host, so boundary atoms land in the same cell), then an
-// LSD radix sort with 8-bit digits whose scatter ranks ties in input order
-// (stable by construction, bit-exact against the CPU sort), then per-cell
-// start offsets by binary search over the sorted keys.
+// is the STABLE sort of atoms by cid.  Here:
+//   1. key_hist_kernel: FP64 cell keys (rounding identical to the host, so
+//      boundary atoms land in the same cell), in-cell fractions, and the
+//      per-tile histogram of the first 8-bit digit;
+//   2. per digit: hist_scan_kernel (exclusive scan of that digit's tile
+//      histograms), then radix_scatter_kernel, which ranks ties in input
+//      order (stable by construction, so bit-exact against the CPU sort) and
+//      counts the NEXT digit of every key at the tile it lands in; the last
+//      pass also gathers the atom records into cell order;
+//   3. cell_start_kernel: first sorted rank of every cell.
+// Integer counts only (their sums do not depend on order).
 #include "spme_kernels.hpp"
 
 namespace spme {
 
-// ---------------------------------------------------------------- keys ---
-// Cell index and in-cell fraction, exactly as SFac::sort computes them
+constexpr int RS_THREADS = 128;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 8;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 1024 keys per tile
+constexpr int RS_BINS = 256;
+constexpr int RS_MAX_PASSES = 4;
+
+// Cell index and in-cell fraction exactly as SFac::sort computes them
 // (sfac.cpp:98-106): u = s*K, n = (int)u, u -= n.  A coordinate that wrapped
 // to exactly 1.0 (Cell::wrap of a tiny negative number) is mapped to its
 // periodic image 0 instead of forming the out-of-range key K.
-__global__ void __launch_bounds__(256) cell_key_kernel(Geom g, int n, const double *__restrict__ x,
-                                                       const double *__restrict__ w,
-                                                       uint32_t *__restrict__ keys,
-                                                       uint32_t *__restrict__ idx,
-                                                       float4 *__restrict__ rec) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
+__device__ __forceinline__ uint32_t cell_key(const Geom &g, double x0, double x1, double x2, float4 &r,
+                                             float w) {
   double s0, s1, s2;
-  frac_coords(g, x[3 * a + 0], x[3 * a + 1], x[3 * a + 2], s0, s1, s2);
-  double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
-         u2 = __dmul_rn(s2, (double)g.K2);
+  frac_coords(g, x0, x1, x2, s0, s1, s2);
+  const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
+               u2 = __dmul_rn(s2, (double)g.K2);
   int n0 = __double2int_rz(u0), n1 = __double2int_rz(u1), n2 = __double2int_rz(u2);
-  double f0 = __dsub_rn(u0, (double)n0), f1 = __dsub_rn(u1, (double)n1),
-         f2 = __dsub_rn(u2, (double)n2);
+  double f0 = __dsub_rn(u0, (double)n0), f1 = __dsub_rn(u1, (double)n1), f2 = __dsub_rn(u2, (double)n2);
   if (n0 >= g.K0) { n0 = 0; f0 = 0.0; }
   if (n1 >= g.K1) { n1 = 0; f1 = 0.0; }
   if (n2 >= g.K2) { n2 = 0; f2 = 0.0; }
-  keys[a] = (uint32_t)((n0 * g.K1 + n1) * g.K2 + n2);
-  idx[a] = (uint32_t)a;
-  rec[a] = make_float4((float)f0, (float)f1, (float)f2, (float)w[a]);
+  r = make_float4((float)f0, (float)f1, (float)f2, w);
+  return (uint32_t)((n0 * g.K1 + n1) * g.K2 + n2);
 }
 
-// ------------------------------------------------------------ radix sort ---
-constexpr int RS_THREADS = 256;
-constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 8;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 2048 keys per tile
-constexpr int RS_BINS = 256;
-
-// Per-tile digit histogram, stored digit-major: hist[d * ntiles + tile].
-__global__ void __launch_bounds__(RS_THREADS) radix_hist_kernel(const uint32_t *__restrict__ keys,
-                                                                int n, int shift,
-                                                                uint32_t *__restrict__ hist,
-                                                                int ntiles) {
-  __shared__ uint32_t h[RS_BINS];
-  h[threadIdx.x] = 0;
+// Keys, records and the first digit's per-tile histogram.  Histograms are
+// stored pass-major then digit-major: hist[(p * 256 + d) * ntiles + tile];
+// the later passes' columns of this tile are zeroed here and filled by the
+// preceding scatter pass.
+// totals[p][d] (zeroed beforehand) receives the global count of digit d of
+// pass p: a permutation-invariant sum, so every pass's digit bases are known
+// after this kernel.
+__global__ void __launch_bounds__(RS_THREADS) key_hist_kernel(Geom g, int n, const double *__restrict__ x,
+                                                              const double *__restrict__ w,
+                                                              uint32_t *__restrict__ keys,
+                                                              float4 *__restrict__ rec,
+                                                              uint32_t *__restrict__ hist, int ntiles,
+                                                              int npass, uint32_t *__restrict__ totals) {
+  __shared__ uint32_t h[RS_MAX_PASSES][RS_BINS];
+  for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_BINS; i += RS_THREADS) (&h[0][0])[i] = 0;
   __syncthreads();
   const int base = blockIdx.x * RS_TILE;
-#pragma unroll
+#pragma unroll 2
   for (int it = 0; it < RS_ITEMS; it++) {
-    int i = base + it * RS_THREADS + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xff], 1u);
+    const int a = base + it * RS_THREADS + threadIdx.x;
+    if (a < n) {
+      float4 r;
+      const uint32_t key = cell_key(g, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
+      keys[a] = key;
+      rec[a] = r;
+      for (int p = 0; p < npass; p++) atomicAdd(&h[p][(key >> (8 * p)) & 0xff], 1u);
+    }
   }
   __syncthreads();
-  hist[threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+  for (int d = threadIdx.x; d < RS_BINS; d += RS_THREADS) {
+    hist[d * ntiles + blockIdx.x] = h[0][d];
+    for (int p = 1; p < npass; p++) hist[(p * RS_BINS + d) * ntiles + blockIdx.x] = 0u;
+    for (int p = 0; p < npass; p++)
+      if (h[p][d]) atomicAdd(&totals[p * RS_BINS + d], h[p][d]);
+  }
 }
 
-// Exclusive scan of `count` entries in place, one block of 1024 threads.
-// Integer sums: the result does not depend on the order of additions.
-__global__ void __launch_bounds__(1024) exclusive_scan_kernel(uint32_t *__restrict__ data, int count) {
-  __shared__ uint32_t part[1024];
-  const int t = threadIdx.x;
-  const int chunk = (count + 1023) / 1024;
-  const int lo = min(count, t * chunk), hi = min(count, lo + chunk);
-  uint32_t s = 0;
-  for (int i = lo; i < hi; i++) s += data[i];
-  part[t] = s;
-  __syncthreads();
-  // Hillis-Steele inclusive scan over the 1024 partial sums.
-  for (int off = 1; off < 1024; off <<= 1) {
-    uint32_t v = (t >= off) ? part[t - off] : 0u;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
+// In place, one block per digit d of one pass:
+//   offsets[d][tile] = sum_{d'<d} totals[d'] + sum_{t<tile} hist[d][t].
+__global__ void __launch_bounds__(256) hist_scan_kernel(uint32_t *__restrict__ hist, int ntiles,
+                                                        const uint32_t *__restrict__ totals) {
+  __shared__ uint32_t wsum[8];
+  __shared__ uint32_t base_s;
+  const int d = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp == 0) {  // base = sum of the totals of smaller digits
+    uint32_t v = 0;
+    for (int e = lane; e < d; e += 32) v += totals[e];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) base_s = v;
   }
-  uint32_t run = (t == 0) ? 0u : part[t - 1];
-  for (int i = lo; i < hi; i++) {
-    uint32_t v = data[i];
-    data[i] = run;
-    run += v;
+  __syncthreads();
+  uint32_t run = base_s;
+  uint32_t *row = hist + (size_t)d * ntiles;
+  for (int t0 = 0; t0 < ntiles; t0 += 256) {
+    const int t = t0 + threadIdx.x;
+    const uint32_t v = (t < ntiles) ? row[t] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0, blk = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t ws = wsum[k];
+      if (k < warp) wpre += ws;
+      blk += ws;
+    }
+    if (t < ntiles) row[t] = run + wpre + incl - v;
+    run += blk;
+    __syncthreads();
   }
 }
 
@@ -93,9 +125,14 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(uint32_t *__restri
 // 32*RS_ITEMS keys of the tile and walks it in memory order; ties inside a
 // round of 32 are ranked by lane, ties across rounds and warps by a running
 // per-warp digit count, ties across tiles by the scanned histogram.
+// vin == nullptr: values are the input positions (first pass).  With
+// hist_next != nullptr the next digit (shift + 8) of every key is counted at
+// the output tile it lands in.  With rec_sorted != nullptr (last pass) the
+// atom record of each key is gathered to its sorted position too.
 __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
     const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin, uint32_t *__restrict__ kout,
-    uint32_t *__restrict__ vout, int n, int shift, const uint32_t *__restrict__ offs, int ntiles) {
+    uint32_t *__restrict__ vout, int n, int shift, const uint32_t *__restrict__ offs, int ntiles,
+    uint32_t *__restrict__ hist_next, const float4 *__restrict__ rec, float4 *__restrict__ rec_sorted) {
   __shared__ uint32_t whist[RS_WARPS][RS_BINS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < RS_WARPS * RS_BINS; i += RS_THREADS) (&whist[0][0])[i] = 0;
@@ -108,7 +145,7 @@ __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
     const int i = base + it * 32 + lane;
     const bool valid = i < n;
     key[it] = valid ? kin[i] : 0u;
-    val[it] = valid ? vin[i] : 0u;
+    val[it] = valid ? (vin ? vin[i] : (uint32_t)i) : 0u;
     const uint32_t d = valid ? ((key[it] >> shift) & 0xff) : RS_BINS;  // sentinel group
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
@@ -121,13 +158,12 @@ __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
     rank[it] = prev + __popc(peers & lt_mask);
   }
   __syncthreads();
-  {  // exclusive prefix over warps, one thread per digit
-    const int d = threadIdx.x;
-    uint32_t run = 0;
+  for (int d = threadIdx.x; d < RS_BINS; d += RS_THREADS) {  // exclusive prefix over warps
+    uint32_t run = offs[d * ntiles + blockIdx.x];
 #pragma unroll
-    for (int w = 0; w < RS_WARPS; w++) {
-      uint32_t c = whist[w][d];
-      whist[w][d] = run;
+    for (int wp = 0; wp < RS_WARPS; wp++) {
+      const uint32_t c = whist[wp][d];
+      whist[wp][d] = run;
       run += c;
     }
   }
@@ -137,70 +173,79 @@ __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
     const int i = base + it * 32 + lane;
     if (i < n) {
       const uint32_t d = (key[it] >> shift) & 0xff;
-      const uint32_t pos = offs[d * ntiles + blockIdx.x] + whist[warp][d] + rank[it];
+      const uint32_t pos = whist[warp][d] + rank[it];
       kout[pos] = key[it];
       vout[pos] = val[it];
+      if (hist_next) atomicAdd(&hist_next[((key[it] >> (shift + 8)) & 0xff) * ntiles + pos / RS_TILE], 1u);
+      if (rec_sorted) rec_sorted[pos] = rec[val[it]];
     }
   }
 }
 
-// rec_sorted[r] = rec[perm[r]]: atom records in cell order.
-__global__ void __launch_bounds__(256) gather_records_kernel(int n, const uint32_t *__restrict__ perm,
-                                                             const float4 *__restrict__ rec,
-                                                             float4 *__restrict__ rec_sorted) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < n) rec_sorted[r] = rec[perm[r]];
-}
-
-// cell_start[c] = first sorted rank whose key >= c, for c in [0, ncell].
-__global__ void __launch_bounds__(256) cell_start_kernel(int n, const uint32_t *__restrict__ keys,
-                                                         long ncell, int *__restrict__ cell_start) {
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c > ncell) return;
+// cell_start[c] = first sorted rank whose key >= c, for c in [0, ncell]; one
+// thread per run of 32 cells (binary search, then a forward walk).
+constexpr int CS_RUN = 32;
+__global__ void __launch_bounds__(256) cell_start_kernel(int n, const uint32_t *__restrict__ keys, long ncell,
+                                                         int *__restrict__ cell_start) {
+  const long c0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * CS_RUN;
+  if (c0 > ncell) return;
   int lo = 0, hi = n;
   while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if ((long)keys[mid] < c) lo = mid + 1; else hi = mid;
+    const int mid = (lo + hi) >> 1;
+    if ((long)keys[mid] < c0) lo = mid + 1; else hi = mid;
   }
-  cell_start[c] = lo;
+  const long c1 = min(c0 + CS_RUN, ncell + 1);
+  for (long c = c0; c < c1; c++) {
+    while (lo < n && (long)keys[lo] < c) lo++;
+    cell_start[c] = lo;
+  }
 }
 
 static int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
-size_t sort_scratch_words(int cap) {
+static int key_passes(long ncell) {
+  int bits = 1;
+  while (bits < 32 && ((ncell - 1) >> bits) > 0) bits++;
+  return (bits + 7) / 8;
+}
+
+size_t sort_scratch_words(int cap, long ncell) {
   const int ntiles = ceil_div(cap > 0 ? cap : 1, RS_TILE);
-  return (size_t)ntiles * RS_BINS;
+  return (size_t)ntiles * RS_BINS * key_passes(ncell) + RS_MAX_PASSES * RS_BINS;
 }
 
 // Computes keys/fractions, sorts, and builds the per-cell offsets.
-// On return (stream order): keys_sorted / perm hold the stable order,
+// On return (stream order): keys[cur] / vals[cur] hold the stable order,
 // rec_sorted the records in that order, cell_start the cell offsets.
 int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
                      cudaStream_t st) {
   const long ncell = (long)g.K0 * g.K1 * g.K2;
   int launches = 0;
+  b.cur = 0;
   if (n > 0) {
-    cell_key_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[0], b.vals[0], b.rec);
-    launches++;
-    int bits = 1;
-    while (bits < 32 && ((ncell - 1) >> bits) > 0) bits++;
+    const int npass = key_passes(ncell);
     const int ntiles = ceil_div(n, RS_TILE);
-    int cur = 0;
-    for (int shift = 0; shift < bits; shift += 8) {
-      radix_hist_kernel<<<ntiles, RS_THREADS, 0, st>>>(b.keys[cur], n, shift, b.hist, ntiles);
-      exclusive_scan_kernel<<<1, 1024, 0, st>>>(b.hist, ntiles * RS_BINS);
-      radix_scatter_kernel<<<ntiles, RS_THREADS, 0, st>>>(b.keys[cur], b.vals[cur], b.keys[cur ^ 1],
-                                                          b.vals[cur ^ 1], n, shift, b.hist, ntiles);
-      cur ^= 1;
-      launches += 3;
-    }
-    b.cur = cur;
-    gather_records_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.vals[cur], b.rec, b.rec_sorted);
+    uint32_t *totals = b.hist + (size_t)ntiles * RS_BINS * npass;
+    cudaMemsetAsync(totals, 0, sizeof(uint32_t) * RS_BINS * npass, st);
+    key_hist_kernel<<<ntiles, RS_THREADS, 0, st>>>(g, n, x, w, b.keys[1], b.rec, b.hist, ntiles, npass, totals);
     launches++;
-  } else {
-    b.cur = 0;
+    // keys live in keys[1] before the first pass; passes alternate 1 -> 0 -> 1 ...
+    int src = 1;
+    for (int p = 0; p < npass; p++) {
+      const int dst = src ^ 1;
+      const bool last = (p == npass - 1);
+      uint32_t *hp = b.hist + (size_t)p * RS_BINS * ntiles;
+      hist_scan_kernel<<<RS_BINS, 256, 0, st>>>(hp, ntiles, totals + p * RS_BINS);
+      radix_scatter_kernel<<<ntiles, RS_THREADS, 0, st>>>(
+          b.keys[src], p == 0 ? nullptr : b.vals[src], b.keys[dst], b.vals[dst], n, 8 * p, hp, ntiles,
+          last ? nullptr : hp + (size_t)RS_BINS * ntiles, b.rec, last ? b.rec_sorted : nullptr);
+      launches += 2;
+      src = dst;
+    }
+    b.cur = src;
   }
-  cell_start_kernel<<<ceil_div(ncell + 1, 256), 256, 0, st>>>(n, b.keys[b.cur], ncell, b.cell_start);
+  cell_start_kernel<<<ceil_div(ceil_div(ncell + 1, CS_RUN), 256), 256, 0, st>>>(n, b.keys[b.cur], ncell,
+                                                                                   b.cell_start);
   return launches + 1;
 }
 

@@ -1,58 +1,196 @@
 // K2: B-spline charge spreading (SFac::operator() + accum_spline,
 // sfac.cpp:113-124,141-168).
 //
-// Owner-computes, like the reference: every grid point is written by exactly
-// one thread, which sums the contributions of the atoms in the order^3
-// neighbouring cells, cells in (i,j,k) order and atoms in sorted order.  No
-// atomics anywhere, so the grid is bit-for-bit reproducible run to run.
+// Owner-computes, like the reference's accum_spline: every grid point has
+// exactly one writer, which adds the contributions of the atoms in its
+// order^3 neighbouring cells in a fixed order.  No atomics, so the grid is
+// bit-for-bit reproducible.
+//
+// Blocking: one CTA owns a 4 x 8 x 32 brick of grid points; in each of its
+// four warps, lane (cx, cy) holds the 32 points of its (x, y) column in
+// registers.  The atoms of the brick's halo (the cells whose stencils reach
+// it) are found through the per-cell offsets of the sorted order; the warps
+// take them in round-robin chunks of 32: each lane stages one atom in shared
+// memory (cell offsets relative to the brick, the order-p B-spline weights
+// of its three fractions, the charge folded into the x weights).  The warp
+// then walks the staged atoms in order: each lane forms its column weight
+// wx*wy and adds wz[t] * (wx*wy) to the p registers the atom's z stencil
+// covers -- the z offset is the same for every lane, so it selects one
+// unrolled code path (a jump table), not a divergent branch.  Finally the
+// four partial bricks are summed in warp order through shared memory and
+// stored with lane = z (coalesced).
 #include "spme_kernels.hpp"
 
 namespace spme {
 
-// One thread per grid point (k1 fastest, so a warp reads 32 consecutive
-// cell offsets per neighbour row: coalesced).
-template <int P>
-__global__ void __launch_bounds__(256) spread_owner_kernel(Geom g, Spline S,
-                                                           const int *__restrict__ cell_start,
-                                                           const float4 *__restrict__ rec,
-                                                           float *__restrict__ grid) {
-  const long npt = (long)g.K0 * g.K1 * g.K2;
-  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= npt) return;
-  const int k1 = (int)(gid % g.K2);
-  const int j1 = (int)((gid / g.K2) % g.K1);
-  const int i1 = (int)(gid / ((long)g.K2 * g.K1));
-  const int h = P / 2;
-  float ans = 0.f;
-#pragma unroll 1
-  for (int i = 0; i < P; i++) {
-    const int xid = imod(i1 - h + i, g.K0) * g.K1;
-#pragma unroll 1
-    for (int j = 0; j < P; j++) {
-      const long yid = (long)(xid + imod(j1 - h + j, g.K1)) * g.K2;
-#pragma unroll
-      for (int k = 0; k < P; k++) {
-        const long cid = yid + imod(k1 - h + k, g.K2);
-        const int r0 = __ldg(cell_start + cid), r1 = __ldg(cell_start + cid + 1);
-        for (int r = r0; r < r1; r++) {
-          const float4 u = __ldg(rec + r);
-          ans += bspl_eval(S, P, u.x, i) * bspl_eval(S, P, u.y, j) * bspl_eval(S, P, u.z, k) * u.w;
-        }
-      }
-    }
+constexpr int SP_TX = 4, SP_TY = 8, SP_TZ = 32;
+constexpr int SP_WARPS = 4;
+
+// acc[Z + t] += w * wz[t] for the t with 0 <= Z + t < TZ (all compile-time).
+template <int P, int Z, int T = 0>
+__device__ __forceinline__ void add_at(float (&acc)[SP_TZ], float w, const float (&wz)[P]) {
+  if constexpr (T < P) {
+    if constexpr (Z + T >= 0 && Z + T < SP_TZ) acc[Z + T] = fmaf(w, wz[T], acc[Z + T]);
+    add_at<P, Z, T + 1>(acc, w, wz);
   }
-  grid[gid] = ans;
 }
 
-int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const float4 *rec_sorted,
-                  float *grid, cudaStream_t st) {
-  const long npt = (long)g.K0 * g.K1 * g.K2;
-  const int blocks = (int)((npt + 255) / 256);
+#define SP_CASE(Z) \
+  case Z:          \
+    add_at<P, Z>(acc, w, wz); \
+    break;
+
+// Dispatch on the warp-uniform stencil offset rz in [-(P-1), SP_TZ-1].
+template <int P>
+__device__ __forceinline__ void z_dispatch(int rz, float (&acc)[SP_TZ], float w, const float (&wz)[P]) {
+  switch (rz) {
+    SP_CASE(-7) SP_CASE(-6) SP_CASE(-5) SP_CASE(-4) SP_CASE(-3) SP_CASE(-2) SP_CASE(-1)
+    SP_CASE(0) SP_CASE(1) SP_CASE(2) SP_CASE(3) SP_CASE(4) SP_CASE(5) SP_CASE(6) SP_CASE(7)
+    SP_CASE(8) SP_CASE(9) SP_CASE(10) SP_CASE(11) SP_CASE(12) SP_CASE(13) SP_CASE(14) SP_CASE(15)
+    SP_CASE(16) SP_CASE(17) SP_CASE(18) SP_CASE(19) SP_CASE(20) SP_CASE(21) SP_CASE(22) SP_CASE(23)
+    SP_CASE(24) SP_CASE(25) SP_CASE(26) SP_CASE(27) SP_CASE(28) SP_CASE(29) SP_CASE(30) SP_CASE(31)
+    default: break;
+  }
+}
+#undef SP_CASE
+
+template <int P>
+struct SpreadSmem {
+  static constexpr int H = P / 2;
+  static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
+  static constexpr int WS = 3 * P + 1;  // staged row stride (odd: no bank conflicts)
+  int start[NR];                         // first sorted atom of each halo row segment
+  int pref[NR + 1];                      // prefix sums of the row segment counts
+  int rel[SP_WARPS][32];                 // staged atom: rx | ry << 8 | (rz + 64) << 16
+  float wt[SP_WARPS][32][WS];            // staged atom: q*M(fx+i), M(fy+j), M(fz+P-1-t)
+  float part[SP_WARPS][SP_TZ][33];       // per-warp partial bricks for the final sum
+};
+
+// One CTA per 4 x 8 x 32 brick; its 4 warps take the brick's staged atoms in
+// round-robin chunks of 32 and keep private register accumulators, summed in
+// warp order at the end (fixed order: deterministic).
+template <int P>
+__global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Spline S, const int *__restrict__ cs,
+                                                                  const uint32_t *__restrict__ keys,
+                                                                  const float4 *__restrict__ rec,
+                                                                  float *__restrict__ grid, int ntx, int nty,
+                                                                  int ntz) {
+  using SM = SpreadSmem<P>;
+  constexpr int H = SM::H, RY = SM::RY, NR = SM::NR;
+  __shared__ SM s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long tile = blockIdx.x;
+  const int tz = (int)(tile % ntz), ty = (int)((tile / ntz) % nty), tx = (int)(tile / ((long)ntz * nty));
+  const int x0 = tx * SP_TX, y0 = ty * SP_TY, z0 = tz * SP_TZ;
+  const int cx = lane >> 3, cy = lane & 7;
+  const int K0 = g.K0, K1 = g.K1, K2 = g.K2;
+
+  float acc[SP_TZ];
+#pragma unroll
+  for (int z = 0; z < SP_TZ; z++) acc[z] = 0.f;
+
+  // extended z cells whose stencils reach [z0, z0 + TZ): [z0 - H, z0 + TZ + H - 2]
+  const int ez_lo = z0 - H, ez_hi = z0 + SP_TZ + H - 2;
+  for (int ezs = ez_lo; ezs <= ez_hi;) {
+    const int n2a = imod(ezs, K2);
+    const int len = min(ez_hi - ezs + 1, K2 - n2a);
+    __syncthreads();  // previous segment's ranges are no longer read
+    // atom ranges of the halo rows for cells [n2a, n2a + len)
+    for (int r = threadIdx.x; r < NR; r += SP_WARPS * 32) {
+      const int ex = x0 - H + r / RY, ey = y0 - H + r % RY;
+      const long base = (long)(imod(ex, K0) * K1 + imod(ey, K1)) * K2 + n2a;
+      const int a0 = __ldg(cs + base), a1 = __ldg(cs + base + len);
+      s.start[r] = a0;
+      s.pref[r + 1] = a1 - a0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int running = 0;
+      for (int c = 0; c < NR; c += 32) {
+        const int r = c + lane;
+        int v = (r < NR) ? s.pref[r + 1] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int u = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += u;
+        }
+        if (r < NR) s.pref[r + 1] = running + v;
+        running += __shfl_sync(0xffffffffu, v, 31);
+      }
+      if (lane == 0) s.pref[0] = 0;
+    }
+    __syncthreads();
+    const int total = s.pref[NR];
+    for (int chunk = warp * 32; chunk < total; chunk += SP_WARPS * 32) {
+      const int t = chunk + lane;
+      if (t < total) {
+        int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s.pref[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        const int a = s.start[lo] + (t - s.pref[lo]);
+        const float4 u = __ldg(rec + a);
+        const int n2 = (int)(__ldg(keys + a) % (uint32_t)K2);
+        const int rx = lo / RY, ry = lo % RY;
+        const int rz = ezs + (n2 - n2a) + H - (P - 1) - z0;
+        s.rel[warp][lane] = rx | (ry << 8) | ((rz + 64) << 16);
+        float *wt = s.wt[warp][lane];
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+          wt[i] = u.w * bspl_eval(S, P, u.x, i);
+          wt[P + i] = bspl_eval(S, P, u.y, i);
+          wt[2 * P + i] = bspl_eval(S, P, u.z, P - 1 - i);
+        }
+      }
+      __syncwarp();
+      const int na = min(32, total - chunk);
+      for (int a = 0; a < na; a++) {
+        const int rel = s.rel[warp][a];
+        const float *wt = s.wt[warp][a];
+        const int i = (rel & 0xff) - cx, j = ((rel >> 8) & 0xff) - cy;
+        const int rz = (rel >> 16) - 64;
+        const bool ok = (unsigned)i < (unsigned)P && (unsigned)j < (unsigned)P;
+        const float w = ok ? wt[ok ? i : 0] * wt[P + (ok ? j : 0)] : 0.f;
+        float wz[P];
+#pragma unroll
+        for (int q = 0; q < P; q++) wz[q] = wt[2 * P + q];
+        z_dispatch<P>(rz, acc, w, wz);
+      }
+      __syncwarp();
+    }
+    ezs += len;
+  }
+
+  // partial bricks to shared memory, then the fixed-order sum over warps
+#pragma unroll
+  for (int z = 0; z < SP_TZ; z++) s.part[warp][z][lane] = acc[z];
+  __syncthreads();
+  const int gz = z0 + lane;
+  for (int c = warp; c < 32; c += SP_WARPS) {
+    const int gx = x0 + (c >> 3), gy = y0 + (c & 7);
+    float v = s.part[0][lane][c];
+#pragma unroll
+    for (int wp = 1; wp < SP_WARPS; wp++) v += s.part[wp][lane][c];
+    if (gx < K0 && gy < K1 && gz < K2) grid[((long)gx * K1 + gy) * K2 + gz] = v;
+  }
+}
+
+template <int P>
+static void spread_p(const Geom &g, const Spline &S, const int *cs, const uint32_t *keys, const float4 *rec,
+                     float *grid, cudaStream_t st) {
+  const int ntx = (g.K0 + SP_TX - 1) / SP_TX, nty = (g.K1 + SP_TY - 1) / SP_TY, ntz = (g.K2 + SP_TZ - 1) / SP_TZ;
+  const long tiles = (long)ntx * nty * ntz;
+  spread_reg_kernel<P><<<(unsigned)tiles, SP_WARPS * 32, 0, st>>>(g, S, cs, keys, rec, grid, ntx, nty, ntz);
+}
+
+int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
+                  const float4 *rec_sorted, float *grid, cudaStream_t st) {
   switch (g.order) {
-    case 2: spread_owner_kernel<2><<<blocks, 256, 0, st>>>(g, S, cell_start, rec_sorted, grid); break;
-    case 4: spread_owner_kernel<4><<<blocks, 256, 0, st>>>(g, S, cell_start, rec_sorted, grid); break;
-    case 6: spread_owner_kernel<6><<<blocks, 256, 0, st>>>(g, S, cell_start, rec_sorted, grid); break;
-    case 8: spread_owner_kernel<8><<<blocks, 256, 0, st>>>(g, S, cell_start, rec_sorted, grid); break;
+    case 2: spread_p<2>(g, S, cell_start, keys_sorted, rec_sorted, grid, st); break;
+    case 4: spread_p<4>(g, S, cell_start, keys_sorted, rec_sorted, grid, st); break;
+    case 6: spread_p<6>(g, S, cell_start, keys_sorted, rec_sorted, grid, st); break;
+    case 8: spread_p<8>(g, S, cell_start, keys_sorted, rec_sorted, grid, st); break;
     default: return 0;
   }
   return 1;

@@ -27,8 +27,10 @@ struct Handle {
   int a_mode = 0;  // 0: no influence function, 1: host tables, 2: Ewald on device
   Influence inf{};
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream all work is enqueued on
+  cudaStream_t own_stream = nullptr;  // the handle's own stream
   cudaEvent_t ev_in = nullptr;
+  cudaEvent_t ev_stage[7] = {};
   // device buffers
   float *d_real = nullptr;
   float2 *d_cplx = nullptr;
@@ -36,7 +38,8 @@ struct Handle {
   float2 *d_tw[3] = {nullptr, nullptr, nullptr};
   FftPlan3 fft{};
   double *d_A = nullptr;  // 7 * nmodes (table mode)
-  double *d_partials = nullptr, *d_red = nullptr;
+  RowImg *d_rows = nullptr;  // K0*K1 row image tables (device Ewald mode)
+  double *d_partials = nullptr, *d_red = nullptr, *d_ev = nullptr;
   int cap = 0;
   double *d_x = nullptr, *d_w = nullptr;
   SortBuffers sb{};
@@ -50,6 +53,21 @@ struct Handle {
   int err = 0;
   char errstr[256] = {0};
   long long launches = 0;
+  // CUDA graph of the device solve, replayed while its key is unchanged
+  unsigned long long version = 1;  // bumped by anything that changes kernel arguments
+  bool use_graph = true;
+  cudaGraphExec_t graph = nullptr;
+  int graph_kernels = 0;
+  struct Key {
+    int n;
+    const void *x, *w, *dx, *phi, *ev;
+    cudaStream_t stream;
+    unsigned long long version;
+    bool operator==(const Key &o) const {
+      return n == o.n && x == o.x && w == o.w && dx == o.dx && phi == o.phi && ev == o.ev &&
+             stream == o.stream && version == o.version;
+    }
+  } gkey{};
 };
 
 Handle *H(void *p) { return reinterpret_cast<Handle *>(p); }
@@ -144,12 +162,13 @@ bool ensure_atoms(Handle *h, int n) {
   bool ok = dalloc(h, &h->d_x, 3 * (size_t)cap) && dalloc(h, &h->d_w, cap);
   for (int i = 0; i < 2; i++) ok = ok && dalloc(h, &h->sb.keys[i], cap) && dalloc(h, &h->sb.vals[i], cap);
   ok = ok && dalloc(h, &h->sb.rec, cap) && dalloc(h, &h->sb.rec_sorted, cap) &&
-       dalloc(h, &h->sb.hist, sort_scratch_words(cap));
+       dalloc(h, &h->sb.hist, sort_scratch_words(cap, h->ncell));
   if (!ok) {
     free_atoms(h);
     return false;
   }
   h->cap = cap;
+  h->version++;  // buffers moved: cached graphs are stale
   return true;
 }
 
@@ -178,7 +197,9 @@ void destroy(Handle *h) {
     dfree(h->d_tw[d]);
   }
   dfree(h->d_A);
+  dfree(h->d_rows);
   dfree(h->d_partials);
+  dfree(h->d_ev);
   dfree(h->d_red);
   dfree(h->sb.cell_start);
   free_atoms(h);
@@ -189,7 +210,10 @@ void destroy(Handle *h) {
   if (h->h_f) cudaFreeHost(h->h_f);
   if (h->h_red) cudaFreeHost(h->h_red);
   if (h->ev_in) cudaEventDestroy(h->ev_in);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  for (auto &e : h->ev_stage)
+    if (e) cudaEventDestroy(e);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
 
@@ -236,11 +260,18 @@ void *sfac_ctor(double L[6], int K[3], int order) {
   g.order = order;
   set_cell(g, L);
   make_spline(order, h->spline, h->nodes);
+  fft_prepare_kernels();
+  if (const char *e = getenv("SFAC_NO_GRAPH")) h->use_graph = !(e[0] && e[0] != '0');
 
-  bool ok = CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) &&
+  bool ok = CK(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) &&
             CK(h, cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+  h->stream = h->own_stream;
+  for (int i = 0; i < 7 && ok; i++) ok = CK(h, cudaEventCreate(&h->ev_stage[i]));
   ok = ok && dalloc(h, &h->d_real, h->nreal) && dalloc(h, &h->d_cplx, h->nmodes) &&
-       dalloc(h, &h->d_partials, (size_t)kConvBlocks * kRedWords) && dalloc(h, &h->d_red, kRedWords) &&
+       dalloc(h, &h->d_partials,
+              (size_t)(fft_x_blocks_max(K[1], K[2]) > kConvBlocks ? fft_x_blocks_max(K[1], K[2]) : kConvBlocks) *
+                  kRedWords) &&
+       dalloc(h, &h->d_red, kRedWords) && dalloc(h, &h->d_ev, kRedWords) &&
        dalloc(h, &h->sb.cell_start, ncell + 1);
   for (int d = 0; d < 3 && ok; d++) ok = dalloc(h, &h->d_iB[d], K[d]) && dalloc(h, &h->d_tw[d], K[d]);
   const size_t hf = (size_t)(2 * h->nmodes > h->nreal ? 2 * h->nmodes : h->nreal);
@@ -282,9 +313,10 @@ void sfac(void *p, int n, const double *w, const double *x) {
   }
   CK(h, cudaEventRecord(h->ev_in, h->stream));
   int k = launch_cell_sort(h->geom, n, h->d_x, h->d_w, h->sb, h->stream);
-  k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.rec_sorted, h->d_real, h->stream);
+  k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real,
+                     h->stream);
   DeconvArgs dc{h->d_iB[0], h->d_iB[1], h->d_iB[2], h->ldim};
-  k += launch_fft_forward(h->fft, h->d_real, h->d_cplx, dc, h->stream);
+  k += launch_fft_forward(h->fft, h->geom, h->d_real, h->d_cplx, dc, h->stream);
   if (!launched(h, k, "sfac kernels")) return;
   // The caller may reuse w and x once this returns: wait for the copies only.
   CK(h, cudaEventSynchronize(h->ev_in));
@@ -321,6 +353,7 @@ void set_L(void *p, double L[6]) {
   Handle *h = H(p);
   if (!h) return;
   set_cell(h->geom, L);
+  h->version++;
 }
 
 // Tabulates A and dA exactly as set_A defines them (sfac.cpp:213-292): every
@@ -384,6 +417,7 @@ int set_A(void *p, rad_fn f, double max_m, void *info) {
   h->inf.A = h->d_A;
   h->inf.dA = h->d_A + nm;
   h->a_mode = 1;
+  h->version++;
   return 0;
 }
 
@@ -398,8 +432,8 @@ double en(void *p) {
     printf("Error: No convolution kernel has been set.\n");
     return 0.0;
   }
-  int k = launch_conv(h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, 0, h->d_partials, h->d_red,
-                      h->stream);
+  int k = launch_energy(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials,
+                        h->d_red, h->stream);
   if (!launched(h, k, "en kernels")) return 0.0;
   if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
       !sync(h))
@@ -418,9 +452,8 @@ double de1(void *p, double vir[6]) {
     printf("Error: No convolution kernel has been set.\n");
     return 0.0;
   }
-  int k = launch_conv(h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, 1, h->d_partials, h->d_red,
-                      h->stream);
-  k += launch_fft_inverse(h->fft, h->d_cplx, h->d_real, h->stream);
+  int k = launch_conv_inverse(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_real,
+                              h->d_partials, h->d_red, h->d_ev, h->stream);
   if (!launched(h, k, "de1 kernels")) return 0.0;
   if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
       !sync(h))
@@ -486,7 +519,111 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   inf.iL22 = h->geom.iL22;
   inf.beta = beta;
   inf.max_m = max_m;
+  inf.K2d = FastDiv((uint32_t)h->K[2]);
+  if (!h->d_rows && !dalloc(h, &h->d_rows, (size_t)h->K[0] * h->K[1])) return 2;
+  inf.rows = h->d_rows;
+  const int k = launch_ewald_rows(h->geom, inf, h->d_rows, h->stream);
+  if (!launched(h, k, "ewald rows") || !sync(h)) return 3;
   h->a_mode = 2;
+  h->version++;
+  return 0;
+}
+
+int sfac_set_stream(void *p, void *stream) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (!sync(h)) return 1;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  h->version++;
+  return 0;
+}
+
+void *sfac_get_stream(void *p) { return p ? (void *)H(p)->stream : nullptr; }
+
+// Full solve on device arrays; with `ev` non-null the stage boundaries are
+// recorded into h->ev_stage.
+static int enqueue_solve(Handle *h, int n, const double *x, const double *w, double *dx, double *phi,
+                         double *ev, bool timed) {
+  cudaStream_t st = h->stream;
+  int k = 0;
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[0], st));
+  k += launch_cell_sort(h->geom, n, x, w, h->sb, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[1], st));
+  k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[2], st));
+  int nb = 0;
+  k += fwd_zy(h->fft, h->d_real, h->d_cplx, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[3], st));
+  k += launch_x_conv(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials, nb, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[4], st));
+  k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->geom.iV, h->d_red, ev, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[5], st));
+  if (n > 0 && (dx || phi)) k += launch_gather(h->geom, h->spline, n, x, w, h->d_real, dx, phi, st);
+  if (timed) CK(h, cudaEventRecord(h->ev_stage[6], st));
+  return k;
+}
+
+static int solve_device(Handle *h, int n, const double *x, const double *w, double *dx, double *phi,
+                        double *ev, bool timed) {
+  if (n < 0 || (n > 0 && (!x || !w)) || !ev) return 1;
+  if (h->a_mode == 0) {
+    printf("Error: No convolution kernel has been set.\n");
+    return 1;
+  }
+  if (!ensure_atoms(h, n)) return 2;
+  if (timed || !h->use_graph) {
+    const int k = enqueue_solve(h, n, x, w, dx, phi, ev, timed);
+    if (!launched(h, k, "solve kernels")) return 3;
+  } else {
+    const Handle::Key key{n, x, w, dx, phi, ev, h->stream, h->version};
+    if (!(h->graph && key == h->gkey)) {
+      if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+      }
+      cudaGraph_t gr = nullptr;
+      if (!CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal))) return 3;
+      const int k = enqueue_solve(h, n, x, w, dx, phi, ev, false);
+      const bool ok_launch = check(h, cudaGetLastError(), "solve kernels (capture)");
+      if (!CK(h, cudaStreamEndCapture(h->stream, &gr)) || !ok_launch) {
+        if (gr) cudaGraphDestroy(gr);
+        return 3;
+      }
+      const bool ok = CK(h, cudaGraphInstantiate(&h->graph, gr, 0));
+      cudaGraphDestroy(gr);
+      if (!ok) {
+        h->graph = nullptr;
+        return 3;
+      }
+      h->gkey = key;
+      h->graph_kernels = k;
+    }
+    if (!CK(h, cudaGraphLaunch(h->graph, h->stream))) return 3;
+    h->launches += h->graph_kernels;
+  }
+  h->last_n = n;
+  h->state = 1;
+  return 0;
+}
+
+int sfac_solve_device(void *p, int n, const double *x, const double *w, double *dx, double *phi, double *ev) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  return solve_device(h, n, x, w, dx, phi, ev, false);
+}
+
+int sfac_solve_device_timed(void *p, int n, const double *x, const double *w, double *dx, double *phi,
+                            double *ev, float stage_ms[6]) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  int rc = solve_device(h, n, x, w, dx, phi, ev, true);
+  if (rc) return rc;
+  if (!sync(h)) return 3;
+  for (int i = 0; i < 6; i++) {
+    float ms = 0.f;
+    if (!CK(h, cudaEventElapsedTime(&ms, h->ev_stage[i], h->ev_stage[i + 1]))) return 3;
+    stage_ms[i] = ms;
+  }
   return 0;
 }
 

@@ -29,6 +29,27 @@ struct Spline {
 
 __host__ __device__ inline int imod(int a, int b) { return ((a % b) + b) % b; }
 
+// Division by a runtime-invariant positive integer d with a multiply-high and
+// a shift (the round-up multiplier method of Granlund and Montgomery): for
+// 0 <= x < 2^31, q = umulhi(x, m) >> s equals x / d exactly.
+struct FastDiv {
+  uint32_t d, m, s;
+  __host__ __device__ FastDiv() : d(1), m(0), s(0) {}
+  __host__ explicit FastDiv(uint32_t d_) : d(d_), m(0), s(0) {
+    if (d <= 1) return;
+    uint32_t l = 0;
+    while ((1ull << l) < d) l++;  // ceil(log2 d)
+    const uint64_t p = 31 + l;
+    m = (uint32_t)(((1ull << p) + d - 1) / d);
+    s = (uint32_t)(p - 32);
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t x) const { return d <= 1 ? x : (__umulhi(x, m) >> s); }
+  __device__ __forceinline__ void divmod(uint32_t x, uint32_t &q, uint32_t &r) const {
+    q = div(x);
+    r = x - q * d;
+  }
+};
+
 // M_n(t + j) by Horner (BSpline::bspl_coef, sfac.hpp:124-131), FP32.
 __device__ __forceinline__ float bspl_eval(const Spline &S, int n, float t, int j) {
   const float *r = S.c + j * n;

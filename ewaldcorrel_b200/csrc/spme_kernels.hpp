@@ -19,18 +19,21 @@ struct SortBuffers {
   int *cell_start;     // K0*K1*K2 + 1 offsets into the sorted order
   int cur;             // which keys/vals buffer holds the sorted result
 };
-size_t sort_scratch_words(int cap);
+size_t sort_scratch_words(int cap, long ncell);
 int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
                       cudaStream_t st);
 
 // ---- spread (k_spread.cu) ----
-int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const float4 *rec_sorted,
-                   float *grid, cudaStream_t st);
+int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
+                  const float4 *rec_sorted, float *grid, cudaStream_t st);
+
+struct Influence;  // defined below (influence function source)
 
 // ---- FFT (k_fft.cu) ----
 struct FftLen {
   int n, nst;
-  int rad[32];
+  int rad[32];       // radix of each stage
+  FastDiv ns[32];    // product of the earlier radices, per stage
   const float2 *tw;  // n twiddles exp(-2 pi i k / n)
 };
 struct FftPlan3 {
@@ -41,9 +44,30 @@ struct DeconvArgs {
   int ldim;
 };
 int fft_make_len(FftLen &L, int n, float2 *tw_dev, cudaStream_t st);
-int launch_fft_forward(const FftPlan3 &F, const float *real, float2 *cplx, const DeconvArgs &dc,
-                        cudaStream_t st);
-int launch_fft_inverse(const FftPlan3 &F, float2 *cplx, float *real, cudaStream_t st);
+void fft_prepare_kernels();  // sets shared-memory limits once (before any graph capture)
+bool fft_plane_fits(int K1, int K2);
+long fft_x_blocks_max(int K1, int K2);  // upper bound of x-pass CTAs (energy/virial partials)
+// sfac path: forward 3D r2c and division by the moduli -> S.
+int launch_fft_forward(const FftPlan3 &F, const Geom &g, const float *real, float2 *cplx, const DeconvArgs &dc,
+                       cudaStream_t st);
+// de1 path: S -> energy/virial (ev, raw sums) and the real potential grid.
+int launch_conv_inverse(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
+                        const double *iB1, const double *iB2, float2 *cplx, float *real, double *partials,
+                        double *raw, double *ev, cudaStream_t st);
+// en path: energy/virial sums of S (raw), same order as launch_conv_inverse.
+int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                  const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st);
+// The three launches of the fused solve, also callable one by one:
+// forward z/y; x forward + convolution + x inverse; inverse y/z (+ reduction).
+int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st);
+int launch_x_conv(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                  const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st);
+int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks, double iV,
+           double *raw, double *ev, cudaStream_t st);
+// fused solve: spread grid -> energy/virial and potential grid.
+int launch_fft_conv_solve(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
+                          const double *iB1, const double *iB2, const float *real_in, float2 *cplx,
+                          float *real_out, double *partials, double *raw, double *ev, cudaStream_t st);
 
 // ---- moduli, influence function, convolution (k_conv.cu) ----
 // M_order(j), j = 0..order-1: the B-spline at the integer nodes (FP64).
@@ -51,6 +75,19 @@ struct SplineNodes {
   double Mj[kMaxOrder];
 };
 int launch_bspline_moduli(int n, int order, const SplineNodes &nodes, double *iB, cudaStream_t st);
+
+// Reciprocal-lattice images of one (kx, ky) row of stored modes: the
+// (i, j) lattice pairs with i = kx mod K0, j = ky mod K1 inside the cutoff
+// sphere, with their x/y components and the z index bounds [k0, k1] of the
+// sphere (set_A's loop bounds, sfac.cpp:240-262).  count < 0: more pairs
+// than fit; the row is then enumerated in full at each use.
+constexpr int kRowPairs = 4;
+struct RowImg {
+  int count;
+  int k0[kRowPairs], k1[kRowPairs];
+  int pad;
+  double mx[kRowPairs], my[kRowPairs], m21[kRowPairs], mz0[kRowPairs];
+};
 
 // Influence function source for the convolution.
 struct Influence {
@@ -60,13 +97,20 @@ struct Influence {
   // mode 2: cell used for m = iL n (the cell current when the kernel was set)
   double iL00, iL10, iL11, iL20, iL21, iL22;
   double beta, max_m;
+  const RowImg *rows;  // mode 2: K0*K1 row image tables (set-up time)
+  FastDiv K2d;         // division by K2
 };
+// Builds the row image tables of an Ewald influence function (mode 2).
+int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStream_t st);
 constexpr int kConvBlocks = 592;  // 4 x 148 SMs: fixed, so the reduction order is fixed
 constexpr int kRedWords = 8;      // e, v00, v11, v22, v10, v20, v21, pad
-// want_scale: 0 = energy only (en); 1 = energy + virial + FQ *= A iB (x2 planes) (de1).
+// Energy/virial sums over S without modifying it (en): raw sums -> out,
+// and ev (may be null).  want_scale = 1 also applies the de1 scaling in place.
 int launch_conv(const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
-                 const double *iB2, float2 *S, int want_scale, double *partials, double *out,
-                 cudaStream_t st);
+                const double *iB2, float2 *S, int want_scale, double *partials, double *out, double *ev,
+                cudaStream_t st);
+// Sum of per-CTA partials -> raw (7) and ev (7), one small kernel.
+int launch_finish(const double *partials, int nblocks, double iV, double *raw, double *ev, cudaStream_t st);
 
 // ---- gather (k_gather.cu) ----
 int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,

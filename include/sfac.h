@@ -92,6 +92,29 @@ const char *sfac_error_string(void *sfac);
 int sfac_device(void *sfac);
 long long sfac_kernel_launches(void *sfac);
 
+/* Run all later work of this handle on `stream` (a cudaStream_t of the
+ * handle's device, e.g. a torch stream); NULL restores the handle's own
+ * stream.  Returns 0. */
+int sfac_set_stream(void *sfac, void *stream);
+void *sfac_get_stream(void *sfac);
+
+/* One full solve on DEVICE arrays, enqueued on the handle's stream without
+ * host copies or synchronisation: cell sort, spread, forward FFT, fused
+ * convolution (energy + virial), inverse FFT, and the gather of dE/dx and
+ * phi at the same points.  x (n*3), w (n), dx (n*3), phi (n) and
+ * ev (7 doubles: E, vir xx, yy, zz, yx, zx, zy) are device pointers; dx
+ * and/or phi may be NULL.  Needs an influence function (set_A or
+ * sfac_set_ewald).  Leaves state 1 (get_S then returns the potential grid).
+ * Returns 0, or nonzero on a bad argument or CUDA error. */
+int sfac_solve_device(void *sfac, int n, const double *x, const double *w, double *dx, double *phi,
+                      double *ev);
+
+/* The same solve with CUDA events between its stages; synchronises and
+ * stores the stage times in stage_ms: [0] cell sort, [1] spread, [2] forward
+ * FFT, [3] convolution, [4] inverse FFT, [5] gather (milliseconds). */
+int sfac_solve_device_timed(void *sfac, int n, const double *x, const double *w, double *dx,
+                            double *phi, double *ev, float stage_ms[6]);
+
 /* Debug views (copies to host; for parity tests).
  * sfac_debug_sort: cell keys and original indices in sorted order (n each)
  *   of the last sfac call.
