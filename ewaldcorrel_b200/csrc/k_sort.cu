@@ -13,6 +13,10 @@
 //      pass also gathers the atom records into cell order;
 //   3. cell_start_kernel: first sorted rank of every cell.
 // Integer counts only (their sums do not depend on order).
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/sfac.h"
 #include "spme_kernels.hpp"
 
 namespace spme {
@@ -250,3 +254,127 @@ int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, Sor
 }
 
 }  // namespace spme
+
+// ---------------------------------------------------------------------------
+// Cell sort that allocates nothing.
+//
+// Some host programs cannot let a library allocate device memory: an MD
+// engine or a serving process that has already handed the whole device to
+// its own memory pool, or a time-critical loop that must never pay for the
+// device-wide synchronisation cudaMalloc and cudaFree imply.  For them,
+// sfac_cell_sort_noalloc() runs the same stable cell sort as sfac() with all
+// of its scratch in one fixed file-scope device array, sized for at most
+// kNoAllocMaxAtoms atoms (about 1.6 MB).  Every GPU that loads this library
+// holds that array until the process exits.  The caller passes the device
+// inputs and outputs.
+namespace {
+
+using namespace spme;
+
+constexpr int kNoAllocMaxAtoms = 1 << 16;
+constexpr int kNoAllocTiles = kNoAllocMaxAtoms / RS_TILE;
+constexpr size_t kNaKeys = 0;                                                  // u32 keys, one side of the ping-pong
+constexpr size_t kNaVals = kNaKeys + sizeof(uint32_t) * kNoAllocMaxAtoms;      // u32 indices, same side
+constexpr size_t kNaRec = kNaVals + sizeof(uint32_t) * kNoAllocMaxAtoms;       // float4 records (not returned)
+constexpr size_t kNaHist = kNaRec + sizeof(float4) * kNoAllocMaxAtoms;         // per-tile digit histograms
+constexpr size_t kNaTotals = kNaHist + sizeof(uint32_t) * RS_MAX_PASSES * RS_BINS * kNoAllocTiles;
+constexpr size_t kNoAllocBytes = kNaTotals + sizeof(uint32_t) * RS_MAX_PASSES * RS_BINS;
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocBytes];
+
+// Device address of g_sort_scratch, looked up once per device (the host-side
+// symbol is only a stand-in: a kernel must be given this address instead).
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+unsigned char *noalloc_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess) {
+      fprintf(stderr, "sfac_cell_sort_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+              cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, const double *x, int *keys,
+                                      int *perm, void *stream) {
+  if (!L || !K || n < 0 || (n > 0 && (!x || !keys || !perm))) {
+    fprintf(stderr, "sfac_cell_sort_noalloc: bad arguments\n");
+    return 1;
+  }
+  if (K[0] < 1 || K[1] < 1 || K[2] < 1 || (long)K[0] * K[1] * K[2] >= 0x7fffffffL) {
+    fprintf(stderr, "sfac_cell_sort_noalloc: bad grid %d %d %d\n", K[0], K[1], K[2]);
+    return 1;
+  }
+  if (n > kNoAllocMaxAtoms) {
+    fprintf(stderr,
+            "sfac_cell_sort_noalloc: %d atoms exceed the fixed scratch capacity of %d atoms "
+            "(use sfac() on a handle for larger systems)\n",
+            n, kNoAllocMaxAtoms);
+    return 1;
+  }
+  if (n == 0) return 0;
+  unsigned char *base = noalloc_scratch();
+  if (!base) return 2;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  // Cell constants with the reference's expressions (sfac.hpp:45-51).
+  Geom g{};
+  g.K0 = K[0];
+  g.K1 = K[1];
+  g.K2 = K[2];
+  g.ldim = K[2] / 2 + 1;
+  g.iV = 1. / (L[0] * L[1] * L[2]);
+  g.iL00 = 1. / L[0];
+  g.iL11 = 1. / L[1];
+  g.iL22 = 1. / L[2];
+  g.iL10 = -L[3] * L[2] * g.iV;
+  g.iL20 = (L[3] * L[5] - L[1] * L[4]) * g.iV;
+  g.iL21 = -L[0] * L[5] * g.iV;
+
+  const long ncell = (long)K[0] * K[1] * K[2];
+  const int npass = key_passes(ncell);
+  const int ntiles = ceil_div(n, RS_TILE);
+  uint32_t *hist = reinterpret_cast<uint32_t *>(base + kNaHist);
+  uint32_t *totals = reinterpret_cast<uint32_t *>(base + kNaTotals);
+  float4 *rec = reinterpret_cast<float4 *>(base + kNaRec);
+  // Ping-pong between the scratch side (0) and the caller's outputs (1),
+  // starting on the side that makes the last pass land in the outputs.
+  uint32_t *kb[2] = {reinterpret_cast<uint32_t *>(base + kNaKeys), reinterpret_cast<uint32_t *>(keys)};
+  uint32_t *vb[2] = {reinterpret_cast<uint32_t *>(base + kNaVals), reinterpret_cast<uint32_t *>(perm)};
+  int src = (npass & 1) ? 0 : 1;
+
+  // The array keeps the previous call's contents: the digit totals must
+  // start at zero (every other scratch word is written before it is read).
+  if (cudaMemsetAsync(totals, 0, sizeof(uint32_t) * RS_BINS * npass, st) != cudaSuccess) return 2;
+  // The records are not returned; x stands in for the weights they carry.
+  key_hist_kernel<<<ntiles, RS_THREADS, 0, st>>>(g, n, x, x, kb[src], rec, hist, ntiles, npass, totals);
+  for (int p = 0; p < npass; p++) {
+    const int dst = src ^ 1;
+    const bool last = (p == npass - 1);
+    uint32_t *hp = hist + (size_t)p * RS_BINS * ntiles;
+    hist_scan_kernel<<<RS_BINS, 256, 0, st>>>(hp, ntiles, totals + p * RS_BINS);
+    radix_scatter_kernel<<<ntiles, RS_THREADS, 0, st>>>(kb[src], p == 0 ? nullptr : vb[src], kb[dst], vb[dst], n,
+                                                        8 * p, hp, ntiles,
+                                                        last ? nullptr : hp + (size_t)RS_BINS * ntiles, rec,
+                                                        nullptr);
+    src = dst;
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "sfac_cell_sort_noalloc: %s\n", cudaGetErrorString(e));
+    return 2;
+  }
+  return 0;
+}

@@ -115,6 +115,25 @@ int sfac_solve_device(void *sfac, int n, const double *x, const double *w, doubl
 int sfac_solve_device_timed(void *sfac, int n, const double *x, const double *w, double *dx,
                             double *phi, double *ev, float stage_ms[6]);
 
+/* Stable cell sort of n atoms that allocates no device memory.  No
+ * counterpart in the reference: it serves host programs that cannot let a
+ * library allocate device memory (the device is already given to their own
+ * memory pool, or their loop must not pay the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  Same keys and order as sfac()'s cell sort
+ * (sfac.cpp:92-111).  L (6) and K (3) are host arrays; x (n*3 doubles) is a
+ * device input, keys and perm (n ints each) are device outputs: the cell key
+ * and the original index of each sorted position.  Work is enqueued on
+ * `stream` (NULL: the default stream); results are valid once it completes.
+ * All scratch lives in one fixed device array per GPU (at most 65,536 atoms,
+ * held until the process exits); larger n is rejected with return code 1.
+ * Every call on a device shares that array and leaves its contents behind,
+ * so calls whose GPU work overlaps (other streams or threads) race.  The
+ * first call on a device looks up the array's device address with that
+ * device current; make it before any stream capture begins.
+ * Returns 0, 1 (bad arguments or n too large), 2 (CUDA error). */
+int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, const double *x, int *keys, int *perm,
+                           void *stream);
+
 /* Debug views (copies to host; for parity tests).
  * sfac_debug_sort: cell keys and original indices in sorted order (n each)
  *   of the last sfac call.
