@@ -2,6 +2,7 @@
 // (set_A, sfac.cpp:213-292; ewald.py:124-132), FP64, and FP64 reductions.
 #pragma once
 
+#include "reduce.cuh"
 #include "spme_kernels.hpp"
 
 namespace spme {
@@ -61,11 +62,6 @@ __device__ __forceinline__ void ewald_images(const Influence &inf, int K0, int K
   }
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
 // Image pairs (i, j) of row (kx, ky) and their z bounds, exactly as
 // ewald_images enumerates them.  Returns the pair count, or -1 when the row
@@ -151,22 +147,8 @@ __device__ __forceinline__ void mode_influence(const Influence &inf, const Geom 
   }
 }
 
-// Deterministic reduction of 7 FP64 per-thread sums over a block: fixed
-// shuffle tree per warp, then warps in order.  Thread c < 7 of warp 0 ends
-// with the block total of component c in out[c] (shared, 8 x 7 doubles).
 __device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*red)[7], double *out_global) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < 7; c++) {
-    const double v = warp_sum(acc[c]);
-    if (lane == 0) red[warp][c] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 7) {
-    double v = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
-    out_global[threadIdx.x] = v;
-  }
+  block_reduce_n<7>(acc, red, out_global);
 }
 
 // Sum of the block partials (warp c sums component c: lanes take blocks in
@@ -176,17 +158,8 @@ __device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*r
 __device__ __forceinline__ void finish_partials(const double *__restrict__ partials, int nblocks, double iV,
                                                 double *__restrict__ raw, double *__restrict__ ev) {
   __shared__ double tot[7];
-  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (c < 7) {
-    double v = 0.0;
-    for (int b = lane; b < nblocks; b += 32) v += partials[(long)b * kRedWords + c];
-    v = warp_sum(v);
-    if (lane == 0) {
-      tot[c] = v;
-      if (raw) raw[c] = v;
-    }
-  }
-  __syncthreads();
+  sum_partials<7>(partials, nblocks, kRedWords, tot);
+  if (raw && threadIdx.x < 7) raw[threadIdx.x] = tot[threadIdx.x];
   if (ev && threadIdx.x == 0) {
     const double fac = iV * iV;
     ev[0] = tot[0] * iV;

@@ -7,74 +7,129 @@
 // the B-spline weights and the order^3 sum are FP32, factorised as
 // sum_i wx_i sum_j wy_j sum_k wz_k Q  (one pass gives phi and all three
 // derivatives).  The chain rule through iL and the scaling are FP64.
+#include "reduce.cuh"
 #include "spme_kernels.hpp"
 
 namespace spme {
 
-template <int P, bool GRAD, bool POT>
+constexpr int kCellWords = 16;  // 9 used: sum_a s_a,i (dE/dr_a)_j
+
+// CELL: also the per-block sums of s_i (dE/dr)_j over the block's points
+// (s = iL^T x, unwrapped), written to cellp[block][9] in a fixed order.
+template <int P, bool GRAD, bool POT, bool CELL>
 __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, const double *__restrict__ x,
                                                      const double *__restrict__ w,
                                                      const float *__restrict__ grid, double *__restrict__ dx,
-                                                     double *__restrict__ phi) {
+                                                     double *__restrict__ phi, double *__restrict__ cellp) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
-  double s0, s1, s2;
-  frac_coords(g, x[3 * a + 0], x[3 * a + 1], x[3 * a + 2], s0, s1, s2);
-  const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
-               u2 = __dmul_rn(s2, (double)g.K2);
-  const int c0 = (int)ceil(u0), c1 = (int)ceil(u1), c2 = (int)ceil(u2);
-  const float t0 = (float)((double)c0 - u0), t1 = (float)((double)c1 - u1), t2 = (float)((double)c2 - u2);
-  const int o0 = imod(c0 - P / 2, g.K0), o1 = imod(c1 - P / 2, g.K1), o2 = imod(c2 - P / 2, g.K2);
-  float wx[P], dwx[P], wy[P], dwy[P], wz[P], dwz[P];
-  int iz[P];
+  double cacc[9];
+  if (CELL) {
 #pragma unroll
-  for (int i = 0; i < P; i++) {
-    dbspl_eval(S, P, t0, i, wx[i], dwx[i]);
-    dbspl_eval(S, P, t1, i, wy[i], dwy[i]);
-    dbspl_eval(S, P, t2, i, wz[i], dwz[i]);
-    iz[i] = (o2 + i) % g.K2;
+    for (int c = 0; c < 9; c++) cacc[c] = 0.0;
   }
-  float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll 1
-  for (int i = 0; i < P; i++) {
-    const long row_x = (long)((o0 + i) % g.K0) * g.K1;
-    float sy = 0.f, dy = 0.f, dz = 0.f;
+  if (a < n) {
+    const double x0 = x[3 * a + 0], x1 = x[3 * a + 1], x2 = x[3 * a + 2];
+    double s0, s1, s2;
+    frac_coords(g, x0, x1, x2, s0, s1, s2);
+    const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
+                 u2 = __dmul_rn(s2, (double)g.K2);
+    const int c0 = (int)ceil(u0), c1 = (int)ceil(u1), c2 = (int)ceil(u2);
+    const float t0 = (float)((double)c0 - u0), t1 = (float)((double)c1 - u1), t2 = (float)((double)c2 - u2);
+    const int o0 = imod(c0 - P / 2, g.K0), o1 = imod(c1 - P / 2, g.K1), o2 = imod(c2 - P / 2, g.K2);
+    float wx[P], dwx[P], wy[P], dwy[P], wz[P], dwz[P];
+    int iz[P];
 #pragma unroll
-    for (int j = 0; j < P; j++) {
-      const float *col = grid + (row_x + (o1 + j) % g.K1) * g.K2;
-      float sz = 0.f, dzz = 0.f;
-#pragma unroll
-      for (int k = 0; k < P; k++) {
-        const float q = __ldg(col + iz[k]);
-        sz = fmaf(wz[k], q, sz);
-        dzz = fmaf(dwz[k], q, dzz);
-      }
-      sy = fmaf(wy[j], sz, sy);
-      dy = fmaf(dwy[j], sz, dy);
-      dz = fmaf(wy[j], dzz, dz);
+    for (int i = 0; i < P; i++) {
+      dbspl_eval(S, P, t0, i, wx[i], dwx[i]);
+      dbspl_eval(S, P, t1, i, wy[i], dwy[i]);
+      dbspl_eval(S, P, t2, i, wz[i], dwz[i]);
+      iz[i] = (o2 + i) % g.K2;
     }
-    pot = fmaf(wx[i], sy, pot);
-    gx = fmaf(dwx[i], sy, gx);
-    gy = fmaf(wx[i], dy, gy);
-    gz = fmaf(wx[i], dz, gz);
+    float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < P; i++) {
+      const long row_x = (long)((o0 + i) % g.K0) * g.K1;
+      float sy = 0.f, dy = 0.f, dz = 0.f;
+#pragma unroll
+      for (int j = 0; j < P; j++) {
+        const float *col = grid + (row_x + (o1 + j) % g.K1) * g.K2;
+        float sz = 0.f, dzz = 0.f;
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+          const float q = __ldg(col + iz[k]);
+          sz = fmaf(wz[k], q, sz);
+          dzz = fmaf(dwz[k], q, dzz);
+        }
+        sy = fmaf(wy[j], sz, sy);
+        dy = fmaf(dwy[j], sz, dy);
+        dz = fmaf(wy[j], dzz, dz);
+      }
+      pot = fmaf(wx[i], sy, pot);
+      gx = fmaf(dwx[i], sy, gx);
+      gy = fmaf(wx[i], dy, gy);
+      gz = fmaf(wx[i], dz, gz);
+    }
+    if (GRAD) {
+      const double f = -w[a] * g.iV;
+      const double G0 = (double)gx * f * g.K0, G1 = (double)gy * f * g.K1, G2 = (double)gz * f * g.K2;
+      const double d0 = g.iL00 * G0;
+      const double d1 = g.iL10 * G0 + g.iL11 * G1;
+      const double d2 = g.iL20 * G0 + g.iL21 * G1 + g.iL22 * G2;
+      dx[3 * a + 0] = d0;
+      dx[3 * a + 1] = d1;
+      dx[3 * a + 2] = d2;
+      if (CELL) {
+        const double v0 = x0 * g.iL00 + x1 * g.iL10 + x2 * g.iL20;  // unwrapped s
+        const double v1 = x1 * g.iL11 + x2 * g.iL21;
+        const double v2 = x2 * g.iL22;
+        cacc[0] = v0 * d0; cacc[1] = v0 * d1; cacc[2] = v0 * d2;
+        cacc[3] = v1 * d0; cacc[4] = v1 * d1; cacc[5] = v1 * d2;
+        cacc[6] = v2 * d0; cacc[7] = v2 * d1; cacc[8] = v2 * d2;
+      }
+    }
+    if (POT) phi[a] = (double)pot * g.iV;
   }
-  if (GRAD) {
-    const double f = -w[a] * g.iV;
-    const double G0 = (double)gx * f * g.K0, G1 = (double)gy * f * g.K1, G2 = (double)gz * f * g.K2;
-    dx[3 * a + 0] = g.iL00 * G0;
-    dx[3 * a + 1] = g.iL10 * G0 + g.iL11 * G1;
-    dx[3 * a + 2] = g.iL20 * G0 + g.iL21 * G1 + g.iL22 * G2;
+  if (CELL) {
+    __shared__ double red[8][9];
+    block_reduce_n<9>(cacc, red, cellp + (long)blockIdx.x * kCellWords);
   }
-  if (POT) phi[a] = (double)pot * g.iV;
+}
+
+// dE/dL (6: [ax, by, cz, bx, cx, cy]) at fixed Cartesian positions:
+//   D = -V iL^T Pi - sum_a s_a (dE/dr_a)^T,  dE/dL = lower triangle of D,
+// Pi the virial (symmetric, from ev[1..6]); the first term is dE/dL at fixed
+// fractional coordinates (notes.tex: V Pi = -(dE/dL)^T L).
+__global__ void cell_grad_kernel(Geom g, const double *__restrict__ cellp, int nblocks,
+                                 const double *__restrict__ ev, double *__restrict__ dEdL) {
+  __shared__ double P9[9];
+  sum_partials<9>(cellp, nblocks, kCellWords, P9);
+  if (threadIdx.x != 0) return;
+  const double iL[3][3] = {{g.iL00, 0.0, 0.0}, {g.iL10, g.iL11, 0.0}, {g.iL20, g.iL21, g.iL22}};
+  const double Pi[3][3] = {{ev[1], ev[4], ev[5]}, {ev[4], ev[2], ev[6]}, {ev[5], ev[6], ev[3]}};
+  const double V = 1.0 / g.iV;
+  double D[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double gs = 0.0;
+      for (int k = 0; k < 3; k++) gs += iL[k][i] * Pi[k][j];
+      D[i][j] = -V * gs - P9[3 * i + j];
+    }
+  dEdL[0] = D[0][0];
+  dEdL[1] = D[1][1];
+  dEdL[2] = D[2][2];
+  dEdL[3] = D[1][0];
+  dEdL[4] = D[2][0];
+  dEdL[5] = D[2][1];
 }
 
 template <int P>
-static int gather_p(const Geom &g, const Spline &S, int n, const double *x, const double *w,
-                     const float *grid, double *dx, double *phi, cudaStream_t st) {
+static int gather_p(const Geom &g, const Spline &S, int n, const double *x, const double *w, const float *grid,
+                    double *dx, double *phi, double *cellp, cudaStream_t st) {
   const int blocks = (n + 255) / 256;
-  if (dx && phi) gather_kernel<P, true, true><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi);
-  else if (dx) gather_kernel<P, true, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi);
-  else if (phi) gather_kernel<P, false, true><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi);
+  if (cellp) gather_kernel<P, true, true, true><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, cellp);
+  else if (dx && phi) gather_kernel<P, true, true, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
+  else if (dx) gather_kernel<P, true, false, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
+  else if (phi) gather_kernel<P, false, true, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
   else return 0;
   return 1;
 }
@@ -83,12 +138,33 @@ int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const 
                   const float *grid, double *dx, double *phi, cudaStream_t st) {
   if (n <= 0) return 0;
   switch (g.order) {
-    case 2: return gather_p<2>(g, S, n, x, w, grid, dx, phi, st);
-    case 4: return gather_p<4>(g, S, n, x, w, grid, dx, phi, st);
-    case 6: return gather_p<6>(g, S, n, x, w, grid, dx, phi, st);
-    case 8: return gather_p<8>(g, S, n, x, w, grid, dx, phi, st);
+    case 2: return gather_p<2>(g, S, n, x, w, grid, dx, phi, nullptr, st);
+    case 4: return gather_p<4>(g, S, n, x, w, grid, dx, phi, nullptr, st);
+    case 6: return gather_p<6>(g, S, n, x, w, grid, dx, phi, nullptr, st);
+    case 8: return gather_p<8>(g, S, n, x, w, grid, dx, phi, nullptr, st);
     default: return 0;
   }
 }
+
+// Gather of dE/dx and phi (phi may be null) plus dE/dL; ev must already hold
+// the energy and virial of this solve.  cellp: ceil(n/256) x kCellWords.
+int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, const double *w,
+                       const float *grid, double *dx, double *phi, double *cellp, const double *ev, double *dEdL,
+                       cudaStream_t st) {
+  int k = 0;
+  if (n > 0) {
+    switch (g.order) {
+      case 2: k = gather_p<2>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
+      case 4: k = gather_p<4>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
+      case 6: k = gather_p<6>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
+      case 8: k = gather_p<8>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
+      default: return 0;
+    }
+  }
+  cell_grad_kernel<<<1, 9 * 32, 0, st>>>(g, cellp, (n + 255) / 256, ev, dEdL);
+  return k + 1;
+}
+
+size_t gather_cell_words(int cap) { return (size_t)((cap + 255) / 256 + 1) * kCellWords; }
 
 }  // namespace spme

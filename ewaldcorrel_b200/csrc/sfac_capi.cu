@@ -45,6 +45,8 @@ struct Handle {
   SortBuffers sb{};
   int gcap = 0;
   double *d_gx = nullptr, *d_gw = nullptr, *d_gout = nullptr;
+  int ccap = 0;
+  double *d_cellp = nullptr;  // per-block partials of the cell adjoint
   int last_n = 0;
   // pinned host buffers
   double *h_S = nullptr;
@@ -60,11 +62,11 @@ struct Handle {
   int graph_kernels = 0;
   struct Key {
     int n;
-    const void *x, *w, *dx, *phi, *ev;
+    const void *x, *w, *dx, *phi, *ev, *dEdL;
     cudaStream_t stream;
     unsigned long long version;
     bool operator==(const Key &o) const {
-      return n == o.n && x == o.x && w == o.w && dx == o.dx && phi == o.phi && ev == o.ev &&
+      return n == o.n && x == o.x && w == o.w && dx == o.dx && phi == o.phi && ev == o.ev && dEdL == o.dEdL &&
              stream == o.stream && version == o.version;
     }
   } gkey{};
@@ -172,6 +174,19 @@ bool ensure_atoms(Handle *h, int n) {
   return true;
 }
 
+bool ensure_cellp(Handle *h, int n) {
+  if (n <= h->ccap && h->d_cellp) return true;
+  dfree(h->d_cellp);
+  const int cap = n + n / 2 + 64;
+  if (!dalloc(h, &h->d_cellp, gather_cell_words(cap))) {
+    h->ccap = 0;
+    return false;
+  }
+  h->ccap = cap;
+  h->version++;
+  return true;
+}
+
 bool ensure_gather(Handle *h, int n) {
   if (n <= h->gcap) return true;
   dfree(h->d_gx);
@@ -206,6 +221,7 @@ void destroy(Handle *h) {
   dfree(h->d_gx);
   dfree(h->d_gw);
   dfree(h->d_gout);
+  dfree(h->d_cellp);
   if (h->h_S) cudaFreeHost(h->h_S);
   if (h->h_f) cudaFreeHost(h->h_f);
   if (h->h_red) cudaFreeHost(h->h_red);
@@ -543,7 +559,7 @@ void *sfac_get_stream(void *p) { return p ? (void *)H(p)->stream : nullptr; }
 // Full solve on device arrays; with `ev` non-null the stage boundaries are
 // recorded into h->ev_stage.
 static int enqueue_solve(Handle *h, int n, const double *x, const double *w, double *dx, double *phi,
-                         double *ev, bool timed) {
+                         double *ev, double *dEdL, bool timed) {
   cudaStream_t st = h->stream;
   int k = 0;
   if (timed) CK(h, cudaEventRecord(h->ev_stage[0], st));
@@ -558,24 +574,28 @@ static int enqueue_solve(Handle *h, int n, const double *x, const double *w, dou
   if (timed) CK(h, cudaEventRecord(h->ev_stage[4], st));
   k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->geom.iV, h->d_red, ev, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[5], st));
-  if (n > 0 && (dx || phi)) k += launch_gather(h->geom, h->spline, n, x, w, h->d_real, dx, phi, st);
+  if (dEdL)
+    k += launch_gather_cell(h->geom, h->spline, n, x, w, h->d_real, dx, phi, h->d_cellp, ev, dEdL, st);
+  else if (n > 0 && (dx || phi))
+    k += launch_gather(h->geom, h->spline, n, x, w, h->d_real, dx, phi, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[6], st));
   return k;
 }
 
 static int solve_device(Handle *h, int n, const double *x, const double *w, double *dx, double *phi,
-                        double *ev, bool timed) {
-  if (n < 0 || (n > 0 && (!x || !w)) || !ev) return 1;
+                        double *ev, double *dEdL, bool timed) {
+  if (n < 0 || (n > 0 && (!x || !w)) || !ev || (dEdL && n > 0 && !dx)) return 1;
   if (h->a_mode == 0) {
     printf("Error: No convolution kernel has been set.\n");
     return 1;
   }
   if (!ensure_atoms(h, n)) return 2;
+  if (dEdL && !ensure_cellp(h, n)) return 2;
   if (timed || !h->use_graph) {
-    const int k = enqueue_solve(h, n, x, w, dx, phi, ev, timed);
+    const int k = enqueue_solve(h, n, x, w, dx, phi, ev, dEdL, timed);
     if (!launched(h, k, "solve kernels")) return 3;
   } else {
-    const Handle::Key key{n, x, w, dx, phi, ev, h->stream, h->version};
+    const Handle::Key key{n, x, w, dx, phi, ev, dEdL, h->stream, h->version};
     if (!(h->graph && key == h->gkey)) {
       if (h->graph) {
         cudaGraphExecDestroy(h->graph);
@@ -583,7 +603,7 @@ static int solve_device(Handle *h, int n, const double *x, const double *w, doub
       }
       cudaGraph_t gr = nullptr;
       if (!CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal))) return 3;
-      const int k = enqueue_solve(h, n, x, w, dx, phi, ev, false);
+      const int k = enqueue_solve(h, n, x, w, dx, phi, ev, dEdL, false);
       const bool ok_launch = check(h, cudaGetLastError(), "solve kernels (capture)");
       if (!CK(h, cudaStreamEndCapture(h->stream, &gr)) || !ok_launch) {
         if (gr) cudaGraphDestroy(gr);
@@ -609,14 +629,21 @@ static int solve_device(Handle *h, int n, const double *x, const double *w, doub
 int sfac_solve_device(void *p, int n, const double *x, const double *w, double *dx, double *phi, double *ev) {
   Handle *h = H(p);
   if (!h) return 1;
-  return solve_device(h, n, x, w, dx, phi, ev, false);
+  return solve_device(h, n, x, w, dx, phi, ev, nullptr, false);
+}
+
+int sfac_solve_device_cell(void *p, int n, const double *x, const double *w, double *dx, double *phi, double *ev,
+                           double *dEdL) {
+  Handle *h = H(p);
+  if (!h || !dEdL) return 1;
+  return solve_device(h, n, x, w, dx, phi, ev, dEdL, false);
 }
 
 int sfac_solve_device_timed(void *p, int n, const double *x, const double *w, double *dx, double *phi,
                             double *ev, float stage_ms[6]) {
   Handle *h = H(p);
   if (!h) return 1;
-  int rc = solve_device(h, n, x, w, dx, phi, ev, true);
+  int rc = solve_device(h, n, x, w, dx, phi, ev, nullptr, true);
   if (rc) return rc;
   if (!sync(h)) return 3;
   for (int i = 0; i < 6; i++) {

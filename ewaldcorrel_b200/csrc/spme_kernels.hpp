@@ -114,6 +114,12 @@ int launch_finish(const double *partials, int nblocks, double iV, double *raw, d
 
 // ---- gather (k_gather.cu) ----
 int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,
-                   const float *grid, double *dx, double *phi, cudaStream_t st);
+                  const float *grid, double *dx, double *phi, cudaStream_t st);
+// Gather + cell adjoint: dE/dL (6 doubles, device) from dE/dx, the virial in ev
+// and the positions; cellp is scratch of gather_cell_words(n) doubles.
+int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, const double *w,
+                       const float *grid, double *dx, double *phi, double *cellp, const double *ev, double *dEdL,
+                       cudaStream_t st);
+size_t gather_cell_words(int cap);
 
 }  // namespace spme

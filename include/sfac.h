@@ -109,6 +109,14 @@ void *sfac_get_stream(void *sfac);
 int sfac_solve_device(void *sfac, int n, const double *x, const double *w, double *dx, double *phi,
                       double *ev);
 
+/* sfac_solve_device plus the derivative of the energy with respect to the
+ * box at fixed Cartesian positions: dEdL (6 doubles, device) in the order of
+ * L = [ax, by, cz, bx, cx, cy].  dx is required (dE/dx feeds the adjoint):
+ *   dE/dL = lower triangle of (-V iL^T Pi - sum_a s_a (dE/dx_a)^T),
+ * Pi the virial, s_a = iL^T x_a.  No counterpart in the reference. */
+int sfac_solve_device_cell(void *sfac, int n, const double *x, const double *w, double *dx, double *phi,
+                           double *ev, double *dEdL);
+
 /* The same solve with CUDA events between its stages; synchronises and
  * stores the stage times in stage_ms: [0] cell sort, [1] spread, [2] forward
  * FFT, [3] convolution, [4] inverse FFT, [5] gather (milliseconds). */
