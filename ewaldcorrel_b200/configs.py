@@ -140,25 +140,41 @@ def cfg4_batch(count: int = 64) -> list:
     return out
 
 
-def cfg5_request(rng) -> System:
-    """One serving request: N log-uniform in [500, 200000] (even), density
-    100 atoms/nm^3, alternating +-1 charges, K = 2/3/5-smooth >= L/0.1 in
-    [24, 128], order 4 or 6, beta 3.12."""
-    n = int(round(math.exp(rng.uniform(math.log(500), math.log(200000)))))
-    n += n % 2
-    side = (n / 100.0) ** (1.0 / 3.0)
-    k = min(128, max(24, smooth_235(int(round(side / 0.1)))))
-    order = int(rng.choice([4, 6]))
-    x = rng.uniform(0.0, side, size=(n, 3))
-    q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
-    beta = 3.12
-    return System(f"req_{n}_{k}_p{order}", x, q, np.array([side, side, side, 0.0, 0.0, 0.0]),
-                  (k, k, k), order, beta, MAX_M_FACTOR * beta)
-
-
-def cfg5_stream(count: int = 10000, seed: int = 5) -> list:
+def cfg5_specs(count: int = 10000, seed: int = 5) -> list:
+    """Serving-stream request shapes: N log-uniform in [500, 200000] (even),
+    density 100 atoms/nm^3 (cubic side (N/100)^(1/3) nm), K = 2/3/5-smooth >=
+    round(side/0.1) clamped to [24, 128], order 4 or 6 uniformly, beta 3.12."""
     rng = np.random.default_rng(seed)
-    return [cfg5_request(rng) for _ in range(count)]
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(500), math.log(200000)))))
+        n += n % 2
+        side = (n / 100.0) ** (1.0 / 3.0)
+        k = min(128, max(24, smooth_235(int(round(side / 0.1)))))
+        order = int(rng.choice([4, 6]))
+        beta = 3.12
+        out.append(dict(id=i, n=n, side=side, K=(k, k, k), order=order, beta=beta, max_m=MAX_M_FACTOR * beta))
+    return out
+
+
+CFG5_POOL_ATOMS = 200000
+
+
+def cfg5_pool(seed: int = 5) -> np.ndarray:
+    """Unit-cube fractional positions shared by all serving requests: request
+    i uses the first N_i of them scaled by its box side."""
+    return np.random.default_rng(10_000 + seed).uniform(0.0, 1.0, size=(CFG5_POOL_ATOMS, 3))
+
+
+def cfg5_charges(n: int) -> np.ndarray:
+    return np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+
+
+def cfg5_request(spec: dict, pool: np.ndarray) -> System:
+    n, side = spec["n"], spec["side"]
+    return System(f"req_{spec['id']}_{n}_{spec['K'][0]}_p{spec['order']}", pool[:n] * side, cfg5_charges(n),
+                  np.array([side, side, side, 0.0, 0.0, 0.0]), spec["K"], spec["order"], spec["beta"],
+                  spec["max_m"])
 
 
 BY_NAME = {

@@ -25,7 +25,7 @@ __device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
 // (sfac.cpp:240-289, same sphere bounds, FP64 without contraction).  The
 // conjugate images that set_A folds onto interior modes have the same f
 // values, so the caller doubles those instead of revisiting them.
-__device__ __forceinline__ void ewald_images(const Influence &inf, int K0, int K1, int K2, int kx, int ky, int kz,
+__device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1, int K2, int kx, int ky, int kz,
                              double &sf, double sd[6]) {
   const double R2 = __dmul_rn(inf.max_m, inf.max_m);
   const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
@@ -66,7 +66,7 @@ __device__ __forceinline__ void ewald_images(const Influence &inf, int K0, int K
 // Image pairs (i, j) of row (kx, ky) and their z bounds, exactly as
 // ewald_images enumerates them.  Returns the pair count, or -1 when the row
 // has more than kRowPairs pairs.
-__device__ __forceinline__ int ewald_row(const Influence &inf, int K0, int K1, int kx, int ky, RowImg &r) {
+__device__ __forceinline__ int ewald_row(const InfConst &inf, int K0, int K1, int kx, int ky, RowImg &r) {
   const double R2 = __dmul_rn(inf.max_m, inf.max_m);
   const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
   int c = 0;
@@ -97,8 +97,8 @@ __device__ __forceinline__ int ewald_row(const Influence &inf, int K0, int K1, i
 
 // Same sums as ewald_images from a row's precomputed pairs: per pair only
 // the z images (k = kz mod K2 within [k0, k1]) and their exp are evaluated.
-__device__ __forceinline__ void ewald_images_row(const Influence &inf, const RowImg &r, int K2, int kz, double &sf,
-                                                 double sd[6]) {
+__device__ __forceinline__ void ewald_images_row(const InfConst &inf, const FastDiv &K2d, const RowImg &r, int K2,
+                                                 int kz, double &sf, double sd[6]) {
   const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
   sf = 0.0;
   for (int c = 0; c < 6; c++) sd[c] = 0.0;
@@ -108,8 +108,8 @@ __device__ __forceinline__ void ewald_images_row(const Influence &inf, const Row
     const double mx = r.mx[c], my = r.my[c], m21 = r.m21[c], mz0 = r.mz0[c];
     // first k >= k0 with k = kz (mod K2)
     const int d = kz - k0;
-    int k = k0 + (d >= 0 ? d - (int)inf.K2d.div((uint32_t)d) * K2
-                         : (K2 - 1) - (int)((uint32_t)(-d - 1) - inf.K2d.div((uint32_t)(-d - 1)) * K2));
+    int k = k0 + (d >= 0 ? d - (int)K2d.div((uint32_t)d) * K2
+                         : (K2 - 1) - (int)((uint32_t)(-d - 1) - K2d.div((uint32_t)(-d - 1)) * K2));
     for (; k <= k1; k += K2) {
       const double mz = __dadd_rn(mz0, __dmul_rn((double)k, inf.iL22));
       const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
@@ -127,8 +127,16 @@ __device__ __forceinline__ void ewald_images_row(const Influence &inf, const Row
 
 // A (with set_A's half weight on the kz = 0 and even-K2 Nyquist planes) and
 // dA (6 components) of stored mode (kx, ky, kz), index i = (kx*K1 + ky)*ldim + kz.
-__device__ __forceinline__ void mode_influence(const Influence &inf, const Geom &g, long i, int kx, int ky,
-                                               int kz, bool plane, double &A, double dA[6]) {
+// The device Ewald constants, or zeros when the influence comes from tables.
+__device__ __forceinline__ InfConst load_ic(const Influence &inf) {
+  InfConst c{};
+  if (inf.mode == 2) c = *inf.ic;
+  return c;
+}
+
+// ic: the device Ewald constants (load_ic(inf)), loaded once by the caller.
+__device__ __forceinline__ void mode_influence(const Influence &inf, const InfConst &ic, const Geom &g, long i, int kx,
+                                               int ky, int kz, bool plane, double &A, double dA[6]) {
   if (inf.mode == 1) {
     A = inf.A[i];
 #pragma unroll
@@ -136,8 +144,8 @@ __device__ __forceinline__ void mode_influence(const Influence &inf, const Geom 
   } else {
     double sf, sd[6];
     const RowImg &r = inf.rows[(long)kx * g.K1 + ky];
-    if (r.count >= 0) ewald_images_row(inf, r, g.K2, kz, sf, sd);
-    else ewald_images(inf, g.K0, g.K1, g.K2, kx, ky, kz, sf, sd);
+    if (r.count >= 0) ewald_images_row(ic, inf.K2d, r, g.K2, kz, sf, sd);
+    else ewald_images(ic, g.K0, g.K1, g.K2, kx, ky, kz, sf, sd);
     // set_A adds f/2 from each image and from each conjugate image
     // (interior modes), and f' m m in full from both.
     const double wA = plane ? 0.5 : 1.0;
@@ -155,10 +163,12 @@ __device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*r
 // a fixed stride, then a fixed shuffle tree), and the final energy/virial
 // ev = [E, vir_xx, vir_yy, vir_zz, vir_yx, vir_zx, vir_zy] as de1 forms them
 // (sfac.cpp:384-395).  Needs >= 7 warps; raw receives the 7 sums.
-__device__ __forceinline__ void finish_partials(const double *__restrict__ partials, int nblocks, double iV,
-                                                double *__restrict__ raw, double *__restrict__ ev) {
+__device__ __forceinline__ void finish_partials(const double *__restrict__ partials, int nblocks,
+                                                const CellConst *__restrict__ cell, double *__restrict__ raw,
+                                                double *__restrict__ ev) {
   __shared__ double tot[7];
   sum_partials<7>(partials, nblocks, kRedWords, tot);
+  const double iV = cell->iV;
   if (raw && threadIdx.x < 7) raw[threadIdx.x] = tot[threadIdx.x];
   if (ev && threadIdx.x == 0) {
     const double fac = iV * iV;

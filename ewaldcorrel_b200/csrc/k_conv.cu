@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const 
   const int ldim = g.ldim, K1 = g.K1;
   const long nm = (long)g.K0 * K1 * ldim;
   const bool even = (g.K2 % 2) == 0;
+  const InfConst ic = load_ic(inf);
   double acc[7];
 #pragma unroll
   for (int c = 0; c < 7; c++) acc[c] = 0.0;
@@ -46,7 +47,7 @@ __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const 
     const double s = (double)q.x * q.x + (double)q.y * q.y;
     const bool plane = (kz == 0) || (even && kz == ldim - 1);
     double A, dA[6];
-    mode_influence(inf, g, i, kx, ky, kz, plane, A, dA);
+    mode_influence(inf, ic, g, i, kx, ky, kz, plane, A, dA);
     acc[0] += s * A;
 #pragma unroll
     for (int c = 0; c < 6; c++) acc[1 + c] += s * dA[c];
@@ -60,9 +61,10 @@ __global__ void __launch_bounds__(256) conv_kernel(Geom g, Influence inf, const 
   block_reduce7(acc, red, partials + (long)blockIdx.x * kRedWords);
 }
 
-__global__ void conv_finish_kernel(const double *__restrict__ partials, int nblocks, double iV,
-                                   double *__restrict__ raw, double *__restrict__ ev) {
-  finish_partials(partials, nblocks, iV, raw, ev);
+__global__ void conv_finish_kernel(const double *__restrict__ partials, int nblocks,
+                                   const CellConst *__restrict__ cell, double *__restrict__ raw,
+                                   double *__restrict__ ev) {
+  finish_partials(partials, nblocks, cell, raw, ev);
 }
 
 int launch_conv(const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
@@ -73,15 +75,16 @@ int launch_conv(const Geom &g, const Influence &inf, const double *iB0, const do
   if (blocks > kConvBlocks) blocks = kConvBlocks;
   if (want_scale) conv_kernel<true><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
   else conv_kernel<false><<<blocks, 256, 0, st>>>(g, inf, iB0, iB1, iB2, S, partials);
-  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, blocks, g.iV, out, ev);
+  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, blocks, g.cell, out, ev);
   return 2;
 }
 
 __global__ void ewald_rows_kernel(Geom g, Influence inf, RowImg *rows) {
   const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= (long)g.K0 * g.K1) return;
+  const InfConst ic = *inf.ic;
   RowImg row;
-  row.count = ewald_row(inf, g.K0, g.K1, (int)(r / g.K1), (int)(r % g.K1), row);
+  row.count = ewald_row(ic, g.K0, g.K1, (int)(r / g.K1), (int)(r % g.K1), row);
   row.pad = 0;
   rows[r] = row;
 }
@@ -92,8 +95,9 @@ int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStr
   return 1;
 }
 
-int launch_finish(const double *partials, int nblocks, double iV, double *raw, double *ev, cudaStream_t st) {
-  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, nblocks, iV, raw, ev);
+int launch_finish(const double *partials, int nblocks, const CellConst *cell, double *raw, double *ev,
+                  cudaStream_t st) {
+  conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, nblocks, cell, raw, ev);
   return 1;
 }
 

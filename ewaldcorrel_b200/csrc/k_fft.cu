@@ -171,10 +171,10 @@ __global__ void __launch_bounds__(512) fft_plane_fwd_kernel(FftLen Ly, FftLen Lz
 __global__ void __launch_bounds__(512) fft_plane_inv_kernel(FftLen Ly, FftLen Lz, const float2 *__restrict__ cin,
                                                             float *__restrict__ rout, int sz,
                                                             const double *__restrict__ partials, int nblocks,
-                                                            double iV, double *__restrict__ raw,
-                                                            double *__restrict__ ev, FastDiv d_nb1,
-                                                            FastDiv d_ldim) {
-  if (partials && blockIdx.x == 0) finish_partials(partials, nblocks, iV, raw, ev);
+                                                            const CellConst *__restrict__ cell,
+                                                            double *__restrict__ raw, double *__restrict__ ev,
+                                                            FastDiv d_nb1, FastDiv d_ldim) {
+  if (partials && blockIdx.x == 0) finish_partials(partials, nblocks, cell, raw, ev);
   extern __shared__ float2 sm[];
   const int K1 = Ly.n, K2 = Lz.n, ldim = K2 / 2 + 1;
   float2 *twy = sm, *twz = twy + K1, *A = twz + K2, *Bf = A + sz;
@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
     __syncthreads();
   } else {
     const bool even = (g.K2 % 2) == 0;
+    const InfConst ic = load_ic(inf);
     double acc[7];
 #pragma unroll
     for (int c = 0; c < 7; c++) acc[c] = 0.0;
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
       double s = (double)q.x * q.x + (double)q.y * q.y;
       if (MODE == XM_FWD_CONV_INV) s *= ib * ib;  // |F iB|^2
       double A, dA[6];
-      mode_influence(inf, g, i, kx, ky, kz, plane, A, dA);
+      mode_influence(inf, ic, g, i, kx, ky, kz, plane, A, dA);
       acc[0] += s * A;
 #pragma unroll
       for (int c = 0; c < 6; c++) acc[1 + c] += s * dA[c];
@@ -364,7 +365,7 @@ bool fft_plane_fits(int K1, int K2) {
   return plane_smem(K1, K2, sz) <= kPlaneSmemMax;
 }
 
-long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 3) / 4; }
+long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 1) / 2; }
 
 // Forward z (r2c) and y transforms: one fused plane kernel when an x-plane
 // fits in shared memory, else one pass per axis.
@@ -393,18 +394,18 @@ int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st) 
 
 // Inverse y and z (c2r) transforms; with `partials`, the energy/virial
 // partials are reduced first (inside the plane kernel when it is used).
-int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks, double iV,
-           double *raw, double *ev, cudaStream_t st) {
+int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks,
+           const CellConst *cell, double *raw, double *ev, cudaStream_t st) {
   const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
   int sz;
   const size_t psm = plane_smem(K1, K2, sz);
   if (psm <= kPlaneSmemMax) {
-    fft_plane_inv_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], cplx, real, sz, partials, nblocks, iV, raw, ev,
-                                               FastDiv((K1 + 1) / 2), FastDiv(ldim));
+    fft_plane_inv_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], cplx, real, sz, partials, nblocks, cell, raw,
+                                               ev, FastDiv((K1 + 1) / 2), FastDiv(ldim));
     return 1;
   }
   int k = 0;
-  if (partials) k += launch_finish(partials, nblocks, iV, raw, ev, st);
+  if (partials) k += launch_finish(partials, nblocks, cell, raw, ev, st);
   int B, bufsz;
   size_t smem;
   const long nl = (long)K0 * ldim;
@@ -426,6 +427,17 @@ static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const 
   int B, bufsz;
   size_t smem;
   fft_shape(g.K0, nl, B, bufsz, smem);
+  if (F.x_lines > 0) {  // tuned value, if its shared memory fits
+    const int Bt = F.x_lines;
+    int bz = g.K0 * (Bt + 1);
+    if (2 * Bt * (g.K0 / 2 + 1) > bz) bz = 2 * Bt * (g.K0 / 2 + 1);
+    const size_t sm = (size_t)(g.K0 + 2 * (size_t)bz) * sizeof(float2);
+    if (sm <= 200 * 1024) {
+      B = Bt;
+      bufsz = bz;
+      smem = sm;
+    }
+  }
   nblocks = (int)((nl + B - 1) / B);
   fft_x_kernel<MODE><<<nblocks, 256, smem, st>>>(F.len[0], g, inf, iB0, iB1, iB2, cplx, B, bufsz, partials,
                                                  FastDiv(B));
@@ -444,14 +456,14 @@ int launch_conv_inverse(const FftPlan3 &F, const Geom &g, const Influence &inf, 
                         double *raw, double *ev, cudaStream_t st) {
   int nb;
   int k = x_pass<XM_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
-  return k + inv_yz(F, cplx, real, partials, nb, g.iV, raw, ev, st);
+  return k + inv_yz(F, cplx, real, partials, nb, g.cell, raw, ev, st);
 }
 
 int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st) {
   int nb;
   x_pass<XM_EN>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
-  return 1 + launch_finish(partials, nb, g.iV, raw, nullptr, st);
+  return 1 + launch_finish(partials, nb, g.cell, raw, nullptr, st);
 }
 
 int launch_x_conv(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
@@ -465,7 +477,7 @@ int launch_fft_conv_solve(const FftPlan3 &F, const Geom &g, const Influence &inf
   int nb;
   int k = fwd_zy(F, real_in, cplx, st);
   k += x_pass<XM_FWD_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
-  return k + inv_yz(F, cplx, real_out, partials, nb, g.iV, raw, ev, st);
+  return k + inv_yz(F, cplx, real_out, partials, nb, g.cell, raw, ev, st);
 }
 
 }  // namespace spme

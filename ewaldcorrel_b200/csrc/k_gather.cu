@@ -28,9 +28,10 @@ __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, co
     for (int c = 0; c < 9; c++) cacc[c] = 0.0;
   }
   if (a < n) {
+    const CellConst cc = *g.cell;
     const double x0 = x[3 * a + 0], x1 = x[3 * a + 1], x2 = x[3 * a + 2];
     double s0, s1, s2;
-    frac_coords(g, x0, x1, x2, s0, s1, s2);
+    frac_coords(cc, x0, x1, x2, s0, s1, s2);
     const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
                  u2 = __dmul_rn(s2, (double)g.K2);
     const int c0 = (int)ceil(u0), c1 = (int)ceil(u1), c2 = (int)ceil(u2);
@@ -70,24 +71,24 @@ __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, co
       gz = fmaf(wx[i], dz, gz);
     }
     if (GRAD) {
-      const double f = -w[a] * g.iV;
+      const double f = -w[a] * cc.iV;
       const double G0 = (double)gx * f * g.K0, G1 = (double)gy * f * g.K1, G2 = (double)gz * f * g.K2;
-      const double d0 = g.iL00 * G0;
-      const double d1 = g.iL10 * G0 + g.iL11 * G1;
-      const double d2 = g.iL20 * G0 + g.iL21 * G1 + g.iL22 * G2;
+      const double d0 = cc.iL00 * G0;
+      const double d1 = cc.iL10 * G0 + cc.iL11 * G1;
+      const double d2 = cc.iL20 * G0 + cc.iL21 * G1 + cc.iL22 * G2;
       dx[3 * a + 0] = d0;
       dx[3 * a + 1] = d1;
       dx[3 * a + 2] = d2;
       if (CELL) {
-        const double v0 = x0 * g.iL00 + x1 * g.iL10 + x2 * g.iL20;  // unwrapped s
-        const double v1 = x1 * g.iL11 + x2 * g.iL21;
-        const double v2 = x2 * g.iL22;
+        const double v0 = x0 * cc.iL00 + x1 * cc.iL10 + x2 * cc.iL20;  // unwrapped s
+        const double v1 = x1 * cc.iL11 + x2 * cc.iL21;
+        const double v2 = x2 * cc.iL22;
         cacc[0] = v0 * d0; cacc[1] = v0 * d1; cacc[2] = v0 * d2;
         cacc[3] = v1 * d0; cacc[4] = v1 * d1; cacc[5] = v1 * d2;
         cacc[6] = v2 * d0; cacc[7] = v2 * d1; cacc[8] = v2 * d2;
       }
     }
-    if (POT) phi[a] = (double)pot * g.iV;
+    if (POT) phi[a] = (double)pot * cc.iV;
   }
   if (CELL) {
     __shared__ double red[8][9];
@@ -104,9 +105,10 @@ __global__ void cell_grad_kernel(Geom g, const double *__restrict__ cellp, int n
   __shared__ double P9[9];
   sum_partials<9>(cellp, nblocks, kCellWords, P9);
   if (threadIdx.x != 0) return;
-  const double iL[3][3] = {{g.iL00, 0.0, 0.0}, {g.iL10, g.iL11, 0.0}, {g.iL20, g.iL21, g.iL22}};
+  const CellConst c = *g.cell;
+  const double iL[3][3] = {{c.iL00, 0.0, 0.0}, {c.iL10, c.iL11, 0.0}, {c.iL20, c.iL21, c.iL22}};
   const double Pi[3][3] = {{ev[1], ev[4], ev[5]}, {ev[4], ev[2], ev[6]}, {ev[5], ev[6], ev[3]}};
-  const double V = 1.0 / g.iV;
+  const double V = 1.0 / c.iV;
   double D[3][3];
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) {

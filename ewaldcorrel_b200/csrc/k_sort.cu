@@ -32,10 +32,10 @@ constexpr int RS_MAX_PASSES = 4;
 // (sfac.cpp:98-106): u = s*K, n = (int)u, u -= n.  A coordinate that wrapped
 // to exactly 1.0 (Cell::wrap of a tiny negative number) is mapped to its
 // periodic image 0 instead of forming the out-of-range key K.
-__device__ __forceinline__ uint32_t cell_key(const Geom &g, double x0, double x1, double x2, float4 &r,
-                                             float w) {
+__device__ __forceinline__ uint32_t cell_key(const Geom &g, const CellConst &c, double x0, double x1, double x2,
+                                             float4 &r, float w) {
   double s0, s1, s2;
-  frac_coords(g, x0, x1, x2, s0, s1, s2);
+  frac_coords(c, x0, x1, x2, s0, s1, s2);
   const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
                u2 = __dmul_rn(s2, (double)g.K2);
   int n0 = __double2int_rz(u0), n1 = __double2int_rz(u1), n2 = __double2int_rz(u2);
@@ -64,12 +64,13 @@ __global__ void __launch_bounds__(RS_THREADS) key_hist_kernel(Geom g, int n, con
   for (int i = threadIdx.x; i < RS_MAX_PASSES * RS_BINS; i += RS_THREADS) (&h[0][0])[i] = 0;
   __syncthreads();
   const int base = blockIdx.x * RS_TILE;
+  const CellConst cc = *g.cell;
 #pragma unroll 2
   for (int it = 0; it < RS_ITEMS; it++) {
     const int a = base + it * RS_THREADS + threadIdx.x;
     if (a < n) {
       float4 r;
-      const uint32_t key = cell_key(g, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
+      const uint32_t key = cell_key(g, cc, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
       keys[a] = key;
       rec[a] = r;
       for (int p = 0; p < npass; p++) atomicAdd(&h[p][(key >> (8 * p)) & 0xff], 1u);
@@ -278,7 +279,8 @@ constexpr size_t kNaVals = kNaKeys + sizeof(uint32_t) * kNoAllocMaxAtoms;      /
 constexpr size_t kNaRec = kNaVals + sizeof(uint32_t) * kNoAllocMaxAtoms;       // float4 records (not returned)
 constexpr size_t kNaHist = kNaRec + sizeof(float4) * kNoAllocMaxAtoms;         // per-tile digit histograms
 constexpr size_t kNaTotals = kNaHist + sizeof(uint32_t) * RS_MAX_PASSES * RS_BINS * kNoAllocTiles;
-constexpr size_t kNoAllocBytes = kNaTotals + sizeof(uint32_t) * RS_MAX_PASSES * RS_BINS;
+constexpr size_t kNaCell = kNaTotals + sizeof(uint32_t) * RS_MAX_PASSES * RS_BINS;  // box constants
+constexpr size_t kNoAllocBytes = kNaCell + 256;
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocBytes];
 
@@ -329,19 +331,18 @@ extern "C" int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, 
   if (!base) return 2;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  // Cell constants with the reference's expressions (sfac.hpp:45-51).
+  // Box constants with the reference's expressions (sfac.hpp:45-51), copied
+  // into the scratch array (the copy of this pageable source completes
+  // before cudaMemcpyAsync returns).
+  const CellConst cell = make_cell(L);
+  CellConst *dcell = reinterpret_cast<CellConst *>(base + kNaCell);
+  if (cudaMemcpyAsync(dcell, &cell, sizeof(cell), cudaMemcpyHostToDevice, st) != cudaSuccess) return 2;
   Geom g{};
   g.K0 = K[0];
   g.K1 = K[1];
   g.K2 = K[2];
   g.ldim = K[2] / 2 + 1;
-  g.iV = 1. / (L[0] * L[1] * L[2]);
-  g.iL00 = 1. / L[0];
-  g.iL11 = 1. / L[1];
-  g.iL22 = 1. / L[2];
-  g.iL10 = -L[3] * L[2] * g.iV;
-  g.iL20 = (L[3] * L[5] - L[1] * L[4]) * g.iV;
-  g.iL21 = -L[0] * L[5] * g.iV;
+  g.cell = dcell;
 
   const long ncell = (long)K[0] * K[1] * K[2];
   const int npass = key_passes(ncell);

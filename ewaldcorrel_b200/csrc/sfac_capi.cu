@@ -20,7 +20,11 @@ namespace {
 struct Handle {
   int order = 0, K[3] = {0, 0, 0}, ldim = 0;
   long nreal = 0, nmodes = 0, ncell = 0;
-  Geom geom{};
+  Geom geom{};            // grid constants + device address of the box constants
+  CellConst hcell{};      // host copy of the current box constants
+  CellConst *d_cell = nullptr;
+  InfConst hic{};         // host copy of the device Ewald constants
+  InfConst *d_ic = nullptr;
   Spline spline{};
   SplineNodes nodes{};
   int state = -1;  // -1: nothing computed, 0: structure factor, 1: potential grid
@@ -101,17 +105,15 @@ void dfree(T *&p) {
   p = nullptr;
 }
 
-// Cell(L): lower-triangular box, its inverse and 1/V, with the reference's
-// expressions and operation order (sfac.hpp:37-52) so that the keys computed
-// from these constants round exactly like the CPU's.
-void set_cell(Geom &g, const double L[6]) {
-  g.iV = 1. / (L[0] * L[1] * L[2]);
-  g.iL00 = 1. / L[0];
-  g.iL11 = 1. / L[1];
-  g.iL22 = 1. / L[2];
-  g.iL10 = -L[3] * L[2] * g.iV;
-  g.iL20 = (L[3] * L[5] - L[1] * L[4]) * g.iV;
-  g.iL21 = -L[0] * L[5] * g.iV;
+bool check(Handle *h, cudaError_t e, const char *what);
+
+// Cell(L) (sfac.hpp:37-52): host copy, then the device copy on the handle's
+// stream (ordered before any later solve; kernel arguments do not change, so
+// captured graphs stay valid).
+bool set_cell(Handle *h, const double L[6]) {
+  h->hcell = make_cell(L);
+  return check(h, cudaMemcpyAsync(h->d_cell, &h->hcell, sizeof(CellConst), cudaMemcpyHostToDevice, h->stream),
+               "set_cell copy");
 }
 
 // Coefficients of the cardinal B-spline pieces: row j, column i holds the
@@ -215,6 +217,8 @@ void destroy(Handle *h) {
   dfree(h->d_rows);
   dfree(h->d_partials);
   dfree(h->d_ev);
+  dfree(h->d_cell);
+  dfree(h->d_ic);
   dfree(h->d_red);
   dfree(h->sb.cell_start);
   free_atoms(h);
@@ -274,7 +278,6 @@ void *sfac_ctor(double L[6], int K[3], int order) {
   g.K2 = K[2];
   g.ldim = h->ldim;
   g.order = order;
-  set_cell(g, L);
   make_spline(order, h->spline, h->nodes);
   fft_prepare_kernels();
   if (const char *e = getenv("SFAC_NO_GRAPH")) h->use_graph = !(e[0] && e[0] != '0');
@@ -287,13 +290,18 @@ void *sfac_ctor(double L[6], int K[3], int order) {
        dalloc(h, &h->d_partials,
               (size_t)(fft_x_blocks_max(K[1], K[2]) > kConvBlocks ? fft_x_blocks_max(K[1], K[2]) : kConvBlocks) *
                   kRedWords) &&
-       dalloc(h, &h->d_red, kRedWords) && dalloc(h, &h->d_ev, kRedWords) &&
+       dalloc(h, &h->d_red, kRedWords) && dalloc(h, &h->d_ev, kRedWords) && dalloc(h, &h->d_cell, 1) &&
+       dalloc(h, &h->d_ic, 1) &&
        dalloc(h, &h->sb.cell_start, ncell + 1);
   for (int d = 0; d < 3 && ok; d++) ok = dalloc(h, &h->d_iB[d], K[d]) && dalloc(h, &h->d_tw[d], K[d]);
   const size_t hf = (size_t)(2 * h->nmodes > h->nreal ? 2 * h->nmodes : h->nreal);
   ok = ok && CK(h, cudaMallocHost((void **)&h->h_S, sizeof(double) * 2 * h->nmodes)) &&
        CK(h, cudaMallocHost((void **)&h->h_f, sizeof(float) * hf)) &&
        CK(h, cudaMallocHost((void **)&h->h_red, sizeof(double) * kRedWords));
+  if (ok) {
+    g.cell = h->d_cell;
+    ok = set_cell(h, L);
+  }
   if (ok) {
     memset(h->h_S, 0, sizeof(double) * 2 * h->nmodes);
     int n = 0;
@@ -368,8 +376,7 @@ double *get_S(void *p) {
 void set_L(void *p, double L[6]) {
   Handle *h = H(p);
   if (!h) return;
-  set_cell(h->geom, L);
-  h->version++;
+  set_cell(h, L);
 }
 
 // Tabulates A and dA exactly as set_A defines them (sfac.cpp:213-292): every
@@ -389,7 +396,7 @@ int set_A(void *p, rad_fn f, double max_m, void *info) {
     return 2;
   }
   double *A = tab.data(), *dA = A + nm;
-  const Geom &g = h->geom;
+  const CellConst &g = h->hcell;
   const double R2 = max_m * max_m;
   const int i0 = (int)(max_m / g.iL00);
   for (int i = -i0; i <= i0; i++) {
@@ -425,6 +432,7 @@ int set_A(void *p, rad_fn f, double max_m, void *info) {
       }
     }
   }
+  const bool fresh = !h->d_A;
   if (!h->d_A && !dalloc(h, &h->d_A, 7 * (size_t)nm)) return 2;
   if (!CK(h, cudaMemcpyAsync(h->d_A, A, sizeof(double) * 7 * nm, cudaMemcpyHostToDevice, h->stream)) || !sync(h))
     return 2;
@@ -432,8 +440,8 @@ int set_A(void *p, rad_fn f, double max_m, void *info) {
   h->inf.mode = 1;
   h->inf.A = h->d_A;
   h->inf.dA = h->d_A + nm;
+  if (fresh || h->a_mode != 1) h->version++;  // kernel arguments changed
   h->a_mode = 1;
-  h->version++;
   return 0;
 }
 
@@ -454,7 +462,7 @@ double en(void *p) {
   if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
       !sync(h))
     return 0.0;
-  return h->h_red[0] * h->geom.iV;
+  return h->h_red[0] * h->hcell.iV;
 }
 
 double de1(void *p, double vir[6]) {
@@ -475,7 +483,7 @@ double de1(void *p, double vir[6]) {
       !sync(h))
     return 0.0;
   const double *r = h->h_red;
-  const double fac = h->geom.iV * h->geom.iV;
+  const double fac = h->hcell.iV * h->hcell.iV;
   vir[0] = (r[1] + r[0]) * fac;
   vir[1] = (r[2] + r[0]) * fac;
   vir[2] = (r[3] + r[0]) * fac;
@@ -483,7 +491,7 @@ double de1(void *p, double vir[6]) {
   vir[4] = r[5] * fac;
   vir[5] = r[6] * fac;
   h->state = 1;
-  return r[0] * h->geom.iV;
+  return r[0] * h->hcell.iV;
 }
 
 static void gather_call(Handle *h, int n, const double *w, const double *x, double *dx, double *phi) {
@@ -524,24 +532,23 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
     printf("sfac_set_ewald: bad beta %g or max_m %g\n", beta, max_m);
     return 1;
   }
+  const bool fresh = !h->d_rows;
+  if (!h->d_rows && !dalloc(h, &h->d_rows, (size_t)h->K[0] * h->K[1])) return 2;
+  const CellConst &c = h->hcell;
+  h->hic = InfConst{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, beta, max_m};
   Influence &inf = h->inf;
   inf = Influence{};
   inf.mode = 2;
-  inf.iL00 = h->geom.iL00;
-  inf.iL10 = h->geom.iL10;
-  inf.iL11 = h->geom.iL11;
-  inf.iL20 = h->geom.iL20;
-  inf.iL21 = h->geom.iL21;
-  inf.iL22 = h->geom.iL22;
-  inf.beta = beta;
-  inf.max_m = max_m;
-  inf.K2d = FastDiv((uint32_t)h->K[2]);
-  if (!h->d_rows && !dalloc(h, &h->d_rows, (size_t)h->K[0] * h->K[1])) return 2;
+  inf.ic = h->d_ic;
   inf.rows = h->d_rows;
+  inf.K2d = FastDiv((uint32_t)h->K[2]);
+  // constants and row tables are rewritten in place on the stream: later
+  // solves see them without new kernel arguments
+  if (!CK(h, cudaMemcpyAsync(h->d_ic, &h->hic, sizeof(InfConst), cudaMemcpyHostToDevice, h->stream))) return 3;
   const int k = launch_ewald_rows(h->geom, inf, h->d_rows, h->stream);
-  if (!launched(h, k, "ewald rows") || !sync(h)) return 3;
+  if (!launched(h, k, "ewald rows")) return 3;
+  if (fresh || h->a_mode != 2) h->version++;
   h->a_mode = 2;
-  h->version++;
   return 0;
 }
 
@@ -572,7 +579,7 @@ static int enqueue_solve(Handle *h, int n, const double *x, const double *w, dou
   if (timed) CK(h, cudaEventRecord(h->ev_stage[3], st));
   k += launch_x_conv(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials, nb, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[4], st));
-  k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->geom.iV, h->d_red, ev, st);
+  k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->d_cell, h->d_red, ev, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[5], st));
   if (dEdL)
     k += launch_gather_cell(h->geom, h->spline, n, x, w, h->d_real, dx, phi, h->d_cellp, ev, dEdL, st);
@@ -652,6 +659,37 @@ int sfac_solve_device_timed(void *p, int n, const double *x, const double *w, do
     stage_ms[i] = ms;
   }
   return 0;
+}
+
+int sfac_set_graphs(void *p, int enable) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  h->use_graph = enable != 0;
+  return 0;
+}
+
+int sfac_set_tuning(void *p, int key, int value) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (key == SFAC_TUNE_X_LINES) {
+    if (value < 0 || value > 64 || (value & (value - 1))) return 1;
+    h->fft.x_lines = value;
+    h->version++;
+    return 0;
+  }
+  return 1;
+}
+
+unsigned long sfac_footprint_bytes(const int K[3], int n) {
+  const size_t K0 = K[0], K1 = K[1], K2 = K[2], ldim = K2 / 2 + 1, nn = (size_t)(n > 0 ? n : 1);
+  const size_t cap = nn + nn / 2 + 64;
+  size_t b = 4 * K0 * K1 * K2 + 8 * K0 * K1 * ldim + 4 * (K0 * K1 * K2 + 1);  // grids + cell offsets
+  b += (K0 + K1 + K2) * 16 + sizeof(RowImg) * K0 * K1;                   // moduli, twiddles, rows
+  b += 8 * (size_t)fft_x_blocks_max(K[1], K[2]) * kRedWords;               // partials
+  b += cap * (24 + 8 + 16 + 16 + 16);                                      // sort buffers, records
+  b += 8 * cap * 8;                                                        // gather staging
+  b += 8 * 2 * K0 * K1 * ldim + 4 * K0 * K1 * K2;                          // host mirrors (pinned)
+  return b;
 }
 
 int sfac_last_error(void *p) { return p ? H(p)->err : -1; }

@@ -14,11 +14,19 @@ namespace spme {
 
 constexpr int kMaxOrder = 8;  // MAX_SPL_ORDER (sfac.hpp:7); enforced here
 
-// Box and grid constants, passed by value to every kernel.
+// Box constants: iL lower triangle (Cell::iL) and 1/V, FP64, computed on the
+// host with the reference's expressions (sfac.hpp:45-51).  Kernels read them
+// from device memory, so a box change is a small copy, not new kernel
+// arguments (a captured CUDA graph stays valid).
+struct CellConst {
+  double iL00, iL10, iL11, iL20, iL21, iL22, iV, pad;
+};
+
+// Grid constants passed by value to every kernel, plus the device address of
+// the box constants.
 struct Geom {
   int K0, K1, K2, ldim, order;
-  // iL lower triangle (Cell::iL) and 1/V, FP64 (host-computed, sfac.hpp:45-51)
-  double iL00, iL10, iL11, iL20, iL21, iL22, iV;
+  const CellConst *cell;
 };
 
 // order x order polynomial table of the cardinal B-spline M_n: row j holds
@@ -80,12 +88,26 @@ __device__ __forceinline__ void dbspl_eval(const Spline &S, int n, float t, int 
 // it on the host: ((x0*a + x1*b) + x2*c), no FMA contraction, then wrap.
 __device__ __forceinline__ double wrap01_rn(double v) { return __dsub_rn(v, floor(v)); }
 
-__device__ __forceinline__ void frac_coords(const Geom &g, double x0, double x1, double x2,
+__device__ __forceinline__ void frac_coords(const CellConst &g, double x0, double x1, double x2,
                                             double &s0, double &s1, double &s2) {
   s0 = wrap01_rn(__dadd_rn(__dadd_rn(__dmul_rn(x0, g.iL00), __dmul_rn(x1, g.iL10)),
                            __dmul_rn(x2, g.iL20)));
   s1 = wrap01_rn(__dadd_rn(__dmul_rn(x1, g.iL11), __dmul_rn(x2, g.iL21)));
   s2 = wrap01_rn(__dmul_rn(x2, g.iL22));
+}
+
+// Host: box constants from L = [ax, by, cz, bx, cx, cy] (Cell, sfac.hpp:37-52),
+// same expressions and operation order, so device keys round like the host's.
+inline CellConst make_cell(const double L[6]) {
+  CellConst c{};
+  c.iV = 1. / (L[0] * L[1] * L[2]);
+  c.iL00 = 1. / L[0];
+  c.iL11 = 1. / L[1];
+  c.iL22 = 1. / L[2];
+  c.iL10 = -L[3] * L[2] * c.iV;
+  c.iL20 = (L[3] * L[5] - L[1] * L[4]) * c.iV;
+  c.iL21 = -L[0] * L[5] * c.iV;
+  return c;
 }
 
 }  // namespace spme

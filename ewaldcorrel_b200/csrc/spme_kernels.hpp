@@ -38,6 +38,7 @@ struct FftLen {
 };
 struct FftPlan3 {
   FftLen len[3];
+  int x_lines = 0;  // lines per CTA of the x pass (0: heuristic); set by the autotuner
 };
 struct DeconvArgs {
   const double *iB0, *iB1, *iB2;  // null: no moduli division
@@ -62,8 +63,8 @@ int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const 
 int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st);
 int launch_x_conv(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st);
-int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks, double iV,
-           double *raw, double *ev, cudaStream_t st);
+int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks,
+           const CellConst *cell, double *raw, double *ev, cudaStream_t st);
 // fused solve: spread grid -> energy/virial and potential grid.
 int launch_fft_conv_solve(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
                           const double *iB1, const double *iB2, const float *real_in, float2 *cplx,
@@ -89,15 +90,20 @@ struct RowImg {
   double mx[kRowPairs], my[kRowPairs], m21[kRowPairs], mz0[kRowPairs];
 };
 
+// Constants of the device Ewald influence function (device memory): the
+// cell used for m = iL n (the one current when the function was set; later
+// box changes do not touch it, as with set_A) and the Ewald parameters.
+struct InfConst {
+  double iL00, iL10, iL11, iL20, iL21, iL22, beta, max_m;
+};
+
 // Influence function source for the convolution.
 struct Influence {
-  int mode;          // 1: FP64 tables A/dA from set_A; 2: Ewald evaluated on the device
-  const double *A;   // mode 1: K0*K1*ldim
-  const double *dA;  // mode 1: 6*K0*K1*ldim
-  // mode 2: cell used for m = iL n (the cell current when the kernel was set)
-  double iL00, iL10, iL11, iL20, iL21, iL22;
-  double beta, max_m;
-  const RowImg *rows;  // mode 2: K0*K1 row image tables (set-up time)
+  int mode;            // 1: FP64 tables A/dA from set_A; 2: Ewald evaluated on the device
+  const double *A;     // mode 1: K0*K1*ldim
+  const double *dA;    // mode 1: 6*K0*K1*ldim
+  const InfConst *ic;  // mode 2: device constants
+  const RowImg *rows;  // mode 2: K0*K1 row image tables (rebuilt when the function is set)
   FastDiv K2d;         // division by K2
 };
 // Builds the row image tables of an Ewald influence function (mode 2).
@@ -110,7 +116,8 @@ int launch_conv(const Geom &g, const Influence &inf, const double *iB0, const do
                 const double *iB2, float2 *S, int want_scale, double *partials, double *out, double *ev,
                 cudaStream_t st);
 // Sum of per-CTA partials -> raw (7) and ev (7), one small kernel.
-int launch_finish(const double *partials, int nblocks, double iV, double *raw, double *ev, cudaStream_t st);
+int launch_finish(const double *partials, int nblocks, const CellConst *cell, double *raw, double *ev,
+                  cudaStream_t st);
 
 // ---- gather (k_gather.cu) ----
 int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,

@@ -1,0 +1,310 @@
+"""Serving SPME solves with continuous batching on one GPU.
+
+``SpmeServer`` wraps the native serving runtime of libsfac.so
+(``spme_server_*`` in include/sfac.h): a persistent pool of solver slots with
+resident grids, moduli, twiddles and influence tables, admission by device
+memory footprint, one stream per slot so that admitted requests overlap on the
+GPU, and CUDA-graph replay of every slot's solve.
+
+``run_stream`` drives it with timed arrivals: requests are submitted as soon
+as they have arrived and a slot (or memory for a new one) is free, completions
+are polled, and per-request latency (arrival to completion) is recorded.
+``autotune`` picks, per (grid, order) shape, the x-FFT lines per CTA from
+per-stage CUDA-event timings.  ``run_plain`` is the baseline: one request at
+a time, its kernels launched one by one (no graph), waited for before the
+next request.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import statistics
+import time
+from collections import deque
+from ctypes import POINTER, c_double, c_float, c_int, c_longlong, c_ulong, c_void_p
+
+import numpy as np
+
+from . import ewald as _ew
+
+_dbl6 = np.ctypeslib.ndpointer(np.float64, shape=(6,), flags="C_CONTIGUOUS")
+_int3 = np.ctypeslib.ndpointer(np.int32, shape=(3,), flags="C_CONTIGUOUS")
+
+
+def _lib():
+    _, _, lib = _ew.describe_sfac()
+    if not getattr(lib, "_serve_declared", False):
+        lib.spme_server_create.argtypes = [c_int, c_double, c_int, c_int]
+        lib.spme_server_create.restype = c_void_p
+        lib.spme_server_destroy.argtypes = [c_void_p]
+        lib.spme_server_destroy.restype = None
+        lib.spme_server_submit.argtypes = [c_void_p, c_longlong, c_int, _int3, c_int, c_double, c_double, _dbl6,
+                                           c_void_p, c_void_p, c_void_p]
+        lib.spme_server_submit.restype = c_int
+        lib.spme_server_poll.argtypes = [c_void_p, POINTER(c_longlong), c_int]
+        lib.spme_server_poll.restype = c_int
+        lib.spme_server_tune.argtypes = [c_void_p, _int3, c_int, c_int]
+        lib.spme_server_tune.restype = c_int
+        lib.spme_server_stats.argtypes = [c_void_p, POINTER(c_double)]
+        lib.spme_server_stats.restype = c_int
+        lib.sfac_set_tuning.argtypes = [c_void_p, c_int, c_int]
+        lib.sfac_set_tuning.restype = c_int
+        lib.sfac_solve_device_timed.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [POINTER(c_float)]
+        lib.sfac_solve_device_timed.restype = c_int
+        lib.sfac_footprint_bytes.argtypes = [_int3, c_int]
+        lib.sfac_footprint_bytes.restype = c_ulong
+        lib._serve_declared = True
+    return lib
+
+
+class Request:
+    """One solve request: host FP64 positions (n, 3), charges (n), box L (6),
+    grid K, B-spline order, Ewald beta and cutoff max_m."""
+
+    __slots__ = ("id", "n", "K", "order", "beta", "max_m", "L", "x", "q")
+
+    def __init__(self, rid, x, q, L, K, order, beta, max_m):
+        self.id = int(rid)
+        self.x, self.q = x, q
+        self.n = int(q.shape[0])
+        self.L = np.ascontiguousarray(L, dtype=np.float64)
+        self.K = np.ascontiguousarray(K, dtype=np.int32)
+        self.order, self.beta, self.max_m = int(order), float(beta), float(max_m)
+
+
+class SpmeServer:
+    def __init__(self, device=0, budget_bytes=32 << 30, max_inflight=32, graphs=True):
+        self.lib = _lib()
+        self.h = self.lib.spme_server_create(int(device), float(budget_bytes), int(max_inflight), 1 if graphs else 0)
+        if not self.h:
+            raise RuntimeError("spme_server_create failed (no CUDA device?)")
+        self._ids = (c_longlong * 1024)()
+
+    def close(self):
+        if self.h:
+            self.lib.spme_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, req: Request, xbuf, out):
+        """0 admitted, 1 busy (retry after poll), 2 error.  xbuf/out: pinned
+        numpy arrays holding the positions and receiving [E, vir, dx, phi]."""
+        return self.lib.spme_server_submit(self.h, req.id, req.n, req.K, req.order, req.beta, req.max_m, req.L,
+                                           xbuf.ctypes.data, req.q.ctypes.data, out.ctypes.data)
+
+    def poll(self):
+        k = self.lib.spme_server_poll(self.h, self._ids, 1024)
+        return [self._ids[i] for i in range(k)]
+
+    def tune(self, K, order, x_lines):
+        self.lib.spme_server_tune(self.h, np.asarray(K, np.int32), int(order), int(x_lines))
+
+    def stats(self):
+        s = (c_double * 8)()
+        self.lib.spme_server_stats(self.h, s)
+        keys = ["slots", "bytes", "solves", "created", "evicted", "errors", "inflight", "budget"]
+        return {k: s[i] for i, k in enumerate(keys)}
+
+
+def _pinned(shape):
+    import torch
+
+    return torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+
+
+class _Buffers:
+    """Pinned host staging: positions and outputs per in-flight request."""
+
+    def __init__(self, count, nmax):
+        self.free = [(_pinned((nmax, 3)), _pinned(7 + 4 * nmax)) for _ in range(count)]
+
+
+def run_stream(server: SpmeServer, requests, arrivals=None, make_x=None, max_inflight=32, keep=None,
+               timeout_s=600.0):
+    """Serves `requests` (list of Request) arriving at `arrivals` seconds
+    (None: all at once).  make_x(req, buf) fills the pinned position buffer
+    (default: copies req.x).  keep: ids whose outputs are returned.
+    Returns (latencies in s, wall time, outputs dict)."""
+    nmax = max(r.n for r in requests)
+    bufs = _Buffers(max_inflight, max(nmax, 1))
+    total = len(requests)
+    arr = np.zeros(total) if arrivals is None else np.asarray(arrivals, dtype=np.float64)
+    lat = np.zeros(total)
+    outs = {}
+    pending = deque()
+    inflight = {}
+    nxt = 0
+    done = 0
+    t0 = time.perf_counter()
+    while done < total:
+        now = time.perf_counter() - t0
+        if now > timeout_s:
+            raise TimeoutError(f"serving stream exceeded {timeout_s} s ({done}/{total} done)")
+        while nxt < total and arr[nxt] <= now:
+            pending.append(nxt)
+            nxt += 1
+        ids = server.poll()
+        if ids:
+            tdone = time.perf_counter() - t0
+            for rid in ids:
+                i, xb, ob = inflight.pop(rid)
+                lat[i] = tdone - arr[i]
+                if keep is not None and rid in keep:
+                    r = requests[i]
+                    outs[rid] = (ob[0], ob[1:7].copy(), ob[7:7 + 3 * r.n].reshape(r.n, 3).copy(),
+                                 ob[7 + 3 * r.n:7 + 4 * r.n].copy())
+                bufs.free.append((xb, ob))
+                done += 1
+        while pending and bufs.free:
+            i = pending[0]
+            r = requests[i]
+            xb, ob = bufs.free[-1]
+            if make_x is not None:
+                make_x(r, xb)
+            else:
+                xb[: r.n] = r.x
+            rc = server.submit(r, xb, ob)
+            if rc == 1:
+                break
+            if rc != 0:
+                raise RuntimeError(f"spme_server_submit failed for request {r.id}")
+            pending.popleft()
+            bufs.free.pop()
+            inflight[r.id] = (i, xb, ob)
+    return lat, time.perf_counter() - t0, outs
+
+
+def run_plain(requests, make_x=None, device=0, warm=True):
+    """Baseline: one request at a time -- copy in, launch the solve's kernels
+    one by one (no graph), copy out, wait -- with resident per-shape solvers
+    (a first pass, untimed, creates them)."""
+    server = SpmeServer(device=device, max_inflight=1, graphs=False)
+    try:
+        if warm:
+            run_stream(server, requests, None, make_x, max_inflight=1)
+        lat, wall, _ = run_stream(server, requests, None, make_x, max_inflight=1)
+    finally:
+        server.close()
+    return lat, wall
+
+
+def autotune(shapes, device=0, candidates=(0, 4, 8, 16, 32), reps=3):
+    """Per (K, order, n) shape: the x-FFT lines per CTA with the fastest
+    convolution stage (median of `reps` CUDA-event timings).  Returns
+    {(K, order): x_lines}."""
+    import torch
+
+    lib = _lib()
+    out = {}
+    dev = torch.device("cuda", device)
+    for K, order, n in shapes:
+        K = tuple(int(k) for k in K)
+        L = np.array([K[0] * 0.1, K[1] * 0.1, K[2] * 0.1, 0, 0, 0], dtype=np.float64)
+        s = _ew.Sfac(L.copy(), np.asarray(K), int(order))
+        s.set_ewald(3.12, 6.0)
+        rng = np.random.default_rng(0)
+        x = torch.tensor(rng.uniform(0, 1, size=(n, 3)) * L[:3], device=dev)
+        q = torch.tensor(np.where(np.arange(n) % 2 == 0, 1.0, -1.0), device=dev)
+        dx = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        phi = torch.empty(n, dtype=torch.float64, device=dev)
+        ev = torch.empty(7, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        best, best_t = 0, float("inf")
+        ms = (c_float * 6)()
+        for c in candidates:
+            if lib.sfac_set_tuning(s._data, 1, int(c)) != 0:
+                continue
+            ts = []
+            for _ in range(reps + 1):
+                lib.sfac_solve_device_timed(s._data, n, x.data_ptr(), q.data_ptr(), dx.data_ptr(), phi.data_ptr(),
+                                            ev.data_ptr(), ms)
+                ts.append(ms[3])
+            t = statistics.median(ts[1:])
+            if t < best_t:
+                best, best_t = c, t
+        out[(K, int(order))] = best
+        del s
+    return out
+
+
+def percentiles(lat):
+    srt = np.sort(np.asarray(lat))
+    if srt.size == 0:
+        return {"p50": None, "p99": None}
+    return {"p50": float(srt[int(0.5 * (srt.size - 1))] * 1e3),
+            "p99": float(srt[min(srt.size - 1, int(math.ceil(0.99 * srt.size)) - 1)] * 1e3),
+            "mean": float(srt.mean() * 1e3)}
+
+
+def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, device=0, tune=True,
+                     budget_bytes=48 << 30, seed=5):
+    """The serving-stream measurement: `count` requests (cfg5 shapes: 500 to
+    200,000 atoms, 24^3 to 128^3 grids, order 4 or 6), served with
+    continuous batching; capacity from a closed-loop pass, then Poisson
+    arrivals at `load` x capacity for latency; the plain path on the first
+    `plain_count` requests.  Returns a dict of results."""
+    import collections
+
+    import torch
+
+    from . import configs
+
+    specs = configs.cfg5_specs(count, seed)
+    pool = configs.cfg5_pool(seed)
+    qpool = _pinned(configs.CFG5_POOL_ATOMS)
+    qpool[:] = configs.cfg5_charges(configs.CFG5_POOL_ATOMS)
+    reqs = [Request(s["id"], None, qpool[: s["n"]], [s["side"], s["side"], s["side"], 0, 0, 0], s["K"], s["order"],
+                    s["beta"], s["max_m"]) for s in specs]
+
+    def make_x(r, buf):
+        np.multiply(pool[: r.n], r.L[0], out=buf[: r.n])
+
+    tunes = {}
+    t_tune = time.perf_counter()
+    if tune:
+        by_shape = collections.defaultdict(list)
+        for r in reqs:
+            by_shape[(tuple(int(k) for k in r.K), r.order)].append(r.n)
+        shapes = [(K, o, int(np.median(ns))) for (K, o), ns in sorted(by_shape.items())]
+        tunes = autotune(shapes, device=device)
+    t_tune = time.perf_counter() - t_tune
+
+    srv = SpmeServer(device=device, budget_bytes=budget_bytes, max_inflight=max_inflight, graphs=True)
+    for (K, o), xl in tunes.items():
+        srv.tune(K, o, xl)
+    torch.cuda.synchronize(device)
+    _, t_warm, _ = run_stream(srv, reqs, None, make_x, max_inflight=max_inflight)  # slots + graphs
+    _, t_cap, _ = run_stream(srv, reqs, None, make_x, max_inflight=max_inflight)
+    capacity = count / t_cap
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / (load * capacity), size=count))
+    lat, t_open, _ = run_stream(srv, reqs, arrivals, make_x, max_inflight=max_inflight)
+    stats = srv.stats()
+    srv.close()
+
+    sample = reqs[:plain_count]
+    plat, t_plain = run_plain(sample, make_x, device=device)
+    plain = len(sample) / t_plain
+    return {
+        "requests": count,
+        "capacity_solves_per_s": capacity,
+        "served_solves_per_s": count / t_open,
+        "offered_load": load,
+        "latency_ms": percentiles(lat),
+        "plain_solves_per_s": plain,
+        "plain_latency_ms": percentiles(plat),
+        "served_over_plain": capacity / plain,
+        "max_inflight": max_inflight,
+        "slots": int(stats["slots"]),
+        "pool_bytes": int(stats["bytes"]),
+        "errors": int(stats["errors"]),
+        "warm_pass_s": t_warm,
+        "autotune_s": t_tune,
+        "autotuned_shapes": len(tunes),
+        "mean_atoms": float(np.mean([r.n for r in reqs])),
+    }

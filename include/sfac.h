@@ -142,6 +142,44 @@ int sfac_solve_device_timed(void *sfac, int n, const double *x, const double *w,
 int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, const double *x, int *keys, int *perm,
                            void *stream);
 
+/* Use (1) or bypass (0) CUDA-graph replay in sfac_solve_device*.
+ * Returns 0. */
+int sfac_set_graphs(void *sfac, int enable);
+
+/* Tuning knobs chosen by an autotuner (0 restores the heuristic):
+ * SFAC_TUNE_X_LINES: x-FFT lines per CTA (power of two, <= 64).
+ * Returns 0, or 1 for an unknown key or bad value. */
+#define SFAC_TUNE_X_LINES 1
+int sfac_set_tuning(void *sfac, int key, int value);
+
+/* Estimated device + pinned-host bytes of a handle with grid K solving n
+ * atoms (for admission by memory footprint). */
+unsigned long sfac_footprint_bytes(const int K[3], int n);
+
+/* ---- serving runtime (server.cu) ----------------------------------------
+ * A persistent solver pool on one GPU.  Requests (host FP64 arrays) are
+ * admitted into slots -- one handle with resident grids, moduli, twiddles
+ * and fixed buffers per (grid, order, Ewald parameters, atom-count bucket)
+ * -- while the pool's device-memory budget allows (idle slots are evicted
+ * least-recently-used first); each slot runs on its own stream, so requests
+ * overlap on the GPU, and replays its solve as a CUDA graph.  Atoms are
+ * padded to the bucket size with zero charges (no effect on results).
+ * spme_server_submit copies nothing synchronously when x, q and out are
+ * pinned; out receives [E, vir(6), dE/dx (3n), phi (n)] once
+ * spme_server_poll has reported the request id.  Returns of submit: 0
+ * admitted, 1 no slot or memory free now (poll, then retry), 2 error.
+ * Not thread-safe: one host thread drives a server. */
+void *spme_server_create(int device, double budget_bytes, int max_inflight, int use_graphs);
+void spme_server_destroy(void *server);
+int spme_server_submit(void *server, long long id, int n, const int K[3], int order, double beta, double max_m,
+                       const double L[6], const double *x, const double *q, double *out);
+int spme_server_poll(void *server, long long *ids, int max_ids);
+/* Sets x-FFT lines per CTA for slots of grid K and order (autotuner result). */
+int spme_server_tune(void *server, const int K[3], int order, int x_lines);
+/* stats[0..7] = slots, bytes in use, solves, slots created, slots evicted,
+ * errors, in flight, budget. */
+int spme_server_stats(void *server, double *stats);
+
 /* Debug views (copies to host; for parity tests).
  * sfac_debug_sort: cell keys and original indices in sorted order (n each)
  *   of the last sfac call.
