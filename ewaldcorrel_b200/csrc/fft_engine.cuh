@@ -177,6 +177,86 @@ __device__ float2 *run_stages(const FftLen &L, float2 *b0, float2 *b1, const flo
   return b0;
 }
 
+// ---- warp-synchronous variant --------------------------------------------
+// One warp transforms the lines (columns) [c0, c0 + nc) of the shared
+// [j][b] arrays on its own: items are spread over its lanes, stages are
+// separated by __syncwarp only.  Bwd divides by the warp's column capacity
+// (>= nc); warps own disjoint columns, so they never wait on one another.
+template <int R, int SIGN>
+__device__ __forceinline__ void stage_w(const float2 *in, float2 *out, const float2 *tw, int n, const FastDiv &Nd,
+                                        const FastDiv &Bwd, int P, int c0, int nc, int lane) {
+  const int m = n / R;
+  const int Ns = (int)Nd.d;
+  const int twstep = n / (Ns * R);
+  const int items = m * (int)Bwd.d;
+  for (int item = lane; item < items; item += 32) {
+    uint32_t j, bl, q, k;
+    Bwd.divmod((uint32_t)item, j, bl);
+    if ((int)bl >= nc) continue;
+    const int b = c0 + (int)bl;
+    Nd.divmod(j, q, k);
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      v[r] = in[(j + r * m) * P + b];
+      if (r > 0) v[r] = cmul(v[r], twid<SIGN>(tw, r * (int)k * twstep));
+    }
+    Bfly<R, SIGN>::run(v, tw, n);
+    const int idxD = (int)(q * Ns * R + k);
+#pragma unroll
+    for (int r = 0; r < R; r++) out[(idxD + r * Ns) * P + b] = v[r];
+  }
+}
+
+template <int SIGN>
+__device__ void stage_any_w(const float2 *in, float2 *out, const float2 *tw, int n, int R, const FastDiv &Nd, int Bw,
+                            int P, int c0, int nc, int lane) {
+  const int m = n / R;
+  const int Ns = (int)Nd.d;
+  const int twstep = n / (Ns * R);
+  const int step = n / R;
+  for (int item = lane; item < m * Bw * R; item += 32) {
+    const int qo = item % R;
+    const int rest = item / R;
+    const int bl = rest % Bw, j = rest / Bw;
+    if (bl >= nc) continue;
+    const int b = c0 + bl;
+    const int k = j % Ns;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int r = 0; r < R; r++) {
+      float2 x = in[(j + r * m) * P + b];
+      x = cmul(x, twid<SIGN>(tw, r * k * twstep));
+      acc = cadd(acc, cmul(x, twid<SIGN>(tw, ((r * qo) % R) * step)));
+    }
+    const int idxD = (j / Ns) * Ns * R + k;
+    out[(idxD + qo * Ns) * P + b] = acc;
+  }
+}
+
+// All stages for one warp's columns; returns the buffer holding the result
+// (the same for every warp: it depends only on the stage count).
+template <int SIGN>
+__device__ float2 *run_stages_w(const FftLen &L, float2 *b0, float2 *b1, const float2 *tw, const FastDiv &Bwd, int P,
+                                int c0, int nc, int lane) {
+  for (int s = 0; s < L.nst; s++) {
+    const int R = L.rad[s];
+    const FastDiv &Nd = L.ns[s];
+    switch (R) {
+      case 2: stage_w<2, SIGN>(b0, b1, tw, L.n, Nd, Bwd, P, c0, nc, lane); break;
+      case 3: stage_w<3, SIGN>(b0, b1, tw, L.n, Nd, Bwd, P, c0, nc, lane); break;
+      case 4: stage_w<4, SIGN>(b0, b1, tw, L.n, Nd, Bwd, P, c0, nc, lane); break;
+      case 5: stage_w<5, SIGN>(b0, b1, tw, L.n, Nd, Bwd, P, c0, nc, lane); break;
+      case 7: stage_w<7, SIGN>(b0, b1, tw, L.n, Nd, Bwd, P, c0, nc, lane); break;
+      default: stage_any_w<SIGN>(b0, b1, tw, L.n, R, Nd, (int)Bwd.d, P, c0, nc, lane); break;
+    }
+    __syncwarp();
+    float2 *t = b0;
+    b0 = b1;
+    b1 = t;
+  }
+  return b0;
+}
+
 __device__ __forceinline__ void load_twiddles(float2 *tw_s, const FftLen &L) {
   for (int i = threadIdx.x; i < L.n; i += blockDim.x) tw_s[i] = L.tw[i];
 }

@@ -132,10 +132,12 @@ __global__ void __launch_bounds__(256) fft_strided_kernel(FftLen L, long nlines,
 // --- fused plane pass, forward: one CTA per x-plane -----------------------
 // z r2c of the plane's K1 real rows (two rows per complex line), then the
 // y transform of its ldim columns, both in shared memory; one read of the
-// real plane, one write of the half-complex plane.
+// real plane, one write of the half-complex plane.  Loads, the r2c unpack
+// and stores are CTA-wide (coalesced); each transform step is
+// warp-synchronous over a warp's own columns (dz / dy: columns per warp).
 __global__ void __launch_bounds__(512) fft_plane_fwd_kernel(FftLen Ly, FftLen Lz, const float *__restrict__ rin,
-                                                            float2 *__restrict__ cout, int sz, FastDiv d_nb1,
-                                                            FastDiv d_ldim) {
+                                                            float2 *__restrict__ cout, int sz, FastDiv dz, FastDiv dy,
+                                                            FastDiv dK2, FastDiv dldim) {
   extern __shared__ float2 sm[];
   const int K1 = Ly.n, K2 = Lz.n, ldim = K2 / 2 + 1;
   float2 *twy = sm, *twz = twy + K1, *A = twz + K2, *Bf = A + sz;
@@ -145,24 +147,42 @@ __global__ void __launch_bounds__(512) fft_plane_fwd_kernel(FftLen Ly, FftLen Lz
   const float *plane = rin + x * K1 * K2;
   float2 *out = cout + x * K1 * ldim;
   const int nb1 = (K1 + 1) / 2, P1 = nb1 + 1, P2 = ldim + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int e = threadIdx.x; e < K1 * K2; e += blockDim.x) {
-    const int y = e / K2, z = e % K2;
+    uint32_t y, z;
+    dK2.divmod((uint32_t)e, y, z);
     reinterpret_cast<float *>(&A[z * P1 + (y >> 1)])[y & 1] = plane[e];
   }
   if (K1 & 1)
     for (int z = threadIdx.x; z < K2; z += blockDim.x) A[z * P1 + nb1 - 1].y = 0.f;
   __syncthreads();
-  float2 *R1 = run_stages<-1>(Lz, A, Bf, twz, d_nb1, P1);
+  {
+    const int c0 = warp * (int)dz.d, nc = min((int)dz.d, nb1 - c0);
+    if (nc > 0) run_stages_w<-1>(Lz, A, Bf, twz, dz, P1, c0, nc, lane);
+  }
+  float2 *R1 = (Lz.nst & 1) ? Bf : A;
   float2 *O = (R1 == A) ? Bf : A;
+  __syncthreads();
   for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) {
-    const int y = e / ldim, k = e % ldim, b = y >> 1;
-    const float2 u = R1[k * P1 + b], v = R1[((K2 - k) % K2) * P1 + b];
+    uint32_t y, k;
+    dldim.divmod((uint32_t)e, y, k);
+    const int b = (int)y >> 1;
+    const float2 u = R1[k * P1 + b], v = R1[((K2 - (int)k) % K2) * P1 + b];
     O[y * P2 + k] = (y & 1) ? make_float2(0.5f * (u.y + v.y), -0.5f * (u.x - v.x))
                             : make_float2(0.5f * (u.x + v.x), 0.5f * (u.y - v.y));
   }
   __syncthreads();
-  float2 *R2 = run_stages<-1>(Ly, O, R1, twy, d_ldim, P2);
-  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) out[e] = R2[(e / ldim) * P2 + e % ldim];
+  {
+    const int c0 = warp * (int)dy.d, nc = min((int)dy.d, ldim - c0);
+    if (nc > 0) run_stages_w<-1>(Ly, O, R1, twy, dy, P2, c0, nc, lane);
+  }
+  float2 *R2 = (Ly.nst & 1) ? R1 : O;
+  __syncthreads();
+  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) {
+    uint32_t y, k;
+    dldim.divmod((uint32_t)e, y, k);
+    out[e] = R2[y * P2 + k];
+  }
 }
 
 // --- fused plane pass, inverse: y transform then z c2r per x-plane -------
@@ -173,7 +193,8 @@ __global__ void __launch_bounds__(512) fft_plane_inv_kernel(FftLen Ly, FftLen Lz
                                                             const double *__restrict__ partials, int nblocks,
                                                             const CellConst *__restrict__ cell,
                                                             double *__restrict__ raw, double *__restrict__ ev,
-                                                            FastDiv d_nb1, FastDiv d_ldim) {
+                                                            FastDiv dz, FastDiv dy, FastDiv dK2, FastDiv dldim,
+                                                            FastDiv dnb1) {
   if (partials && blockIdx.x == 0) finish_partials(partials, nblocks, cell, raw, ev);
   extern __shared__ float2 sm[];
   const int K1 = Ly.n, K2 = Lz.n, ldim = K2 / 2 + 1;
@@ -184,51 +205,68 @@ __global__ void __launch_bounds__(512) fft_plane_inv_kernel(FftLen Ly, FftLen Lz
   const float2 *in = cin + x * K1 * ldim;
   float *plane = rout + x * K1 * K2;
   const int nb1 = (K1 + 1) / 2, P1 = nb1 + 1, P2 = ldim + 1;
-  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) A[(e / ldim) * P2 + e % ldim] = in[e];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = threadIdx.x; e < K1 * ldim; e += blockDim.x) {
+    uint32_t y, k;
+    dldim.divmod((uint32_t)e, y, k);
+    A[y * P2 + k] = in[e];
+  }
   __syncthreads();
-  float2 *R = run_stages<+1>(Ly, A, Bf, twy, d_ldim, P2);
+  {
+    const int c0 = warp * (int)dy.d, nc = min((int)dy.d, ldim - c0);
+    if (nc > 0) run_stages_w<+1>(Ly, A, Bf, twy, dy, P2, c0, nc, lane);
+  }
+  float2 *R = (Ly.nst & 1) ? Bf : A;
   float2 *O = (R == A) ? Bf : A;
+  __syncthreads();
   // complex lines z = X_{2b} + i X_{2b+1} over the full K2 (Hermitian
   // extension; self-conjugate bins contribute their real part only)
   for (int e = threadIdx.x; e < K2 * nb1; e += blockDim.x) {
-    const int b = e % nb1, k = e / nb1;
-    const int kk = (k < ldim) ? k : K2 - k;
+    uint32_t k, b;
+    dnb1.divmod((uint32_t)e, k, b);
+    const int kk = ((int)k < ldim) ? (int)k : K2 - (int)k;
     const bool selfc = (kk == 0) || (2 * kk == K2);
     float2 a = R[(2 * b) * P2 + kk];
-    float2 c = (2 * b + 1 < K1) ? R[(2 * b + 1) * P2 + kk] : make_float2(0.f, 0.f);
+    float2 c = ((int)(2 * b + 1) < K1) ? R[(2 * b + 1) * P2 + kk] : make_float2(0.f, 0.f);
     if (selfc) {
       a.y = 0.f;
       c.y = 0.f;
     }
-    O[k * P1 + b] = (k < ldim) ? make_float2(a.x - c.y, a.y + c.x) : make_float2(a.x + c.y, c.x - a.y);
+    O[k * P1 + b] = ((int)k < ldim) ? make_float2(a.x - c.y, a.y + c.x) : make_float2(a.x + c.y, c.x - a.y);
   }
   __syncthreads();
-  float2 *R2 = run_stages<+1>(Lz, O, R, twz, d_nb1, P1);
+  {
+    const int c0 = warp * (int)dz.d, nc = min((int)dz.d, nb1 - c0);
+    if (nc > 0) run_stages_w<+1>(Lz, O, R, twz, dz, P1, c0, nc, lane);
+  }
+  float2 *R2 = (Lz.nst & 1) ? R : O;
+  __syncthreads();
   for (int e = threadIdx.x; e < K1 * K2; e += blockDim.x) {
-    const int y = e / K2, z = e % K2;
+    uint32_t y, z;
+    dK2.divmod((uint32_t)e, y, z);
     const float2 v = R2[z * P1 + (y >> 1)];
     plane[e] = (y & 1) ? v.y : v.x;
   }
 }
 
 // --- x pass with the pointwise reciprocal step ---------------------------
-// Lines (ky, kz) of length K0 (stride K1*ldim), B per CTA.
+// Lines (ky, kz) of length K0 (stride K1*ldim), B per CTA, B/8 per warp.
 //   XM_FWD_DECONV : forward, then S = F iB0 iB1 iB2          (sfac, sfac.cpp:125-138)
 //   XM_CONV_INV   : S given; energy/virial sums of |S|^2, S *= A iB (x2 on the
 //                   kz = 0 / even-K2 Nyquist planes), inverse (de1, sfac.cpp:357-392)
 //   XM_FWD_CONV_INV: forward, then the same with S = F iB, inverse (fused solve)
-// Energy/virial sums are FP64, reduced per CTA in a fixed order into
-// partials[blockIdx.x].
 //   XM_EN         : S given; the energy/virial sums only (en, sfac.cpp:304-325),
 //                   with exactly XM_CONV_INV's blocks and per-thread order, so
 //                   en() and de1() return the same energy bit for bit.
+// Energy/virial sums are FP64, reduced per CTA in a fixed order (lane tree,
+// then warps in order) into partials[blockIdx.x].
 enum { XM_FWD_DECONV = 0, XM_CONV_INV = 1, XM_FWD_CONV_INV = 2, XM_EN = 3 };
 
 template <int MODE>
 __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence inf, const double *__restrict__ iB0,
                                                     const double *__restrict__ iB1, const double *__restrict__ iB2,
                                                     float2 *__restrict__ data, int B, int bufsz,
-                                                    double *__restrict__ partials, FastDiv Bd) {
+                                                    double *__restrict__ partials, FastDiv Bd, FastDiv Bwd) {
   extern __shared__ float2 sm[];
   __shared__ double red[8][7];
   const int n = L.n, P = B + 1, ldim = g.ldim, K1 = g.K1;
@@ -237,34 +275,45 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
   load_twiddles(tw, L);
   const long line0 = (long)blockIdx.x * B;
   for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
-    const int b = e % B, j = e / B;
+    uint32_t j, b;
+    Bd.divmod((uint32_t)e, j, b);
     const long line = line0 + b;
     b0[j * P + b] = (line < nlines) ? data[line + j * nlines] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2 *cur = b0;
-  if (MODE == XM_FWD_DECONV || MODE == XM_FWD_CONV_INV) cur = run_stages<-1>(L, b0, b1, tw, Bd, P);
-  float2 *oth = (cur == b0) ? b1 : b0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bw = (int)Bwd.d, c0 = warp * bw;
+  float2 *cur = b0, *oth = b1;
+  if (MODE == XM_FWD_DECONV || MODE == XM_FWD_CONV_INV) {
+    run_stages_w<-1>(L, b0, b1, tw, Bwd, P, c0, bw, lane);
+    if (L.nst & 1) {
+      cur = b1;
+      oth = b0;
+    }
+  }
   if (MODE == XM_FWD_DECONV) {
-    for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
-      const int b = e % B, j = e / B;
+    for (int e = lane; e < bw * n; e += 32) {
+      uint32_t j, bl;
+      Bwd.divmod((uint32_t)e, j, bl);
+      const int b = c0 + (int)bl;
       const long line = line0 + b;
       if (line >= nlines) continue;
       const int ky = (int)(line / ldim), kz = (int)(line % ldim);
       cur[j * P + b] = cscale(cur[j * P + b], (float)(iB0[j] * iB1[ky] * iB2[kz]));
     }
-    __syncthreads();
   } else {
     const bool even = (g.K2 % 2) == 0;
     const InfConst ic = load_ic(inf);
     double acc[7];
 #pragma unroll
     for (int c = 0; c < 7; c++) acc[c] = 0.0;
-    for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
-      const int b = e % B, j = e / B;
+    for (int e = lane; e < bw * n; e += 32) {
+      uint32_t j, bl;
+      Bwd.divmod((uint32_t)e, j, bl);
+      const int b = c0 + (int)bl;
       const long line = line0 + b;
       if (line >= nlines) continue;
-      const int ky = (int)(line / ldim), kz = (int)(line % ldim), kx = j;
+      const int ky = (int)(line / ldim), kz = (int)(line % ldim), kx = (int)j;
       const long i = ((long)kx * K1 + ky) * ldim + kz;
       const bool plane = (kz == 0) || (even && kz == ldim - 1);
       const float2 q = cur[j * P + b];
@@ -282,13 +331,27 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
         cur[j * P + b] = cscale(q, (float)t);
       }
     }
-    block_reduce7(acc, red, partials + (long)blockIdx.x * kRedWords);
-    if (MODE == XM_EN) return;
-    __syncthreads();
-    cur = run_stages<+1>(L, cur, oth, tw, Bd, P);
+#pragma unroll
+    for (int c = 0; c < 7; c++) {
+      const double v = warp_sum(acc[c]);
+      if (lane == 0) red[warp][c] = v;
+    }
+    if (MODE != XM_EN) {
+      __syncwarp();
+      run_stages_w<+1>(L, cur, oth, tw, Bwd, P, c0, bw, lane);
+      if (L.nst & 1) cur = oth;
+    }
   }
+  __syncthreads();
+  if (MODE != XM_FWD_DECONV && threadIdx.x < 7) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
+    partials[(long)blockIdx.x * kRedWords + threadIdx.x] = v;
+  }
+  if (MODE == XM_EN) return;
   for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
-    const int b = e % B, j = e / B;
+    uint32_t j, b;
+    Bd.divmod((uint32_t)e, j, b);
     const long line = line0 + b;
     if (line < nlines) data[line + j * nlines] = cur[j * P + b];
   }
@@ -365,7 +428,7 @@ bool fft_plane_fits(int K1, int K2) {
   return plane_smem(K1, K2, sz) <= kPlaneSmemMax;
 }
 
-long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 1) / 2; }
+long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 7) / 8; }
 
 // Forward z (r2c) and y transforms: one fused plane kernel when an x-plane
 // fits in shared memory, else one pass per axis.
@@ -374,8 +437,9 @@ int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st) 
   int sz;
   const size_t psm = plane_smem(K1, K2, sz);
   if (psm <= kPlaneSmemMax) {
-    fft_plane_fwd_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], real, cplx, sz, FastDiv((K1 + 1) / 2),
-                                               FastDiv(ldim));
+    const int nb1 = (K1 + 1) / 2;
+    fft_plane_fwd_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], real, cplx, sz, FastDiv((nb1 + 15) / 16),
+                                               FastDiv((ldim + 15) / 16), FastDiv(K2), FastDiv(ldim));
     return 1;
   }
   int B, bufsz;
@@ -400,8 +464,10 @@ int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials,
   int sz;
   const size_t psm = plane_smem(K1, K2, sz);
   if (psm <= kPlaneSmemMax) {
+    const int nb1 = (K1 + 1) / 2;
     fft_plane_inv_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], cplx, real, sz, partials, nblocks, cell, raw,
-                                               ev, FastDiv((K1 + 1) / 2), FastDiv(ldim));
+                                               ev, FastDiv((nb1 + 15) / 16), FastDiv((ldim + 15) / 16), FastDiv(K2),
+                                               FastDiv(ldim), FastDiv(nb1));
     return 1;
   }
   int k = 0;
@@ -420,27 +486,38 @@ int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials,
   return k + 2;
 }
 
+// Lines per CTA of the x pass: 8 warps x bw lines; bw is the smallest power
+// of two giving every lane a butterfly in the first stage, halved while the
+// pass would have under two CTAs per SM (148 SMs); x_lines overrides it.
+static int x_lines_per_cta(const FftPlan3 &F, int n, long nlines) {
+  int B = (F.x_lines + 7) / 8 * 8;
+  if (B <= 0) {
+    const int m = F.len[0].nst > 0 ? n / F.len[0].rad[0] : n;
+    int bw = 1;
+    while (bw < 8 && m * bw < 32) bw <<= 1;
+    while (bw > 1 && (nlines + 8 * bw - 1) / (8 * bw) < 2 * 148) bw >>= 1;
+    B = 8 * bw;
+  }
+  if (B < 8) B = 8;
+  return B;
+}
+
 template <int MODE>
 static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st) {
   const long nl = (long)g.K1 * g.ldim;
-  int B, bufsz;
-  size_t smem;
-  fft_shape(g.K0, nl, B, bufsz, smem);
-  if (F.x_lines > 0) {  // tuned value, if its shared memory fits
-    const int Bt = F.x_lines;
-    int bz = g.K0 * (Bt + 1);
-    if (2 * Bt * (g.K0 / 2 + 1) > bz) bz = 2 * Bt * (g.K0 / 2 + 1);
-    const size_t sm = (size_t)(g.K0 + 2 * (size_t)bz) * sizeof(float2);
-    if (sm <= 200 * 1024) {
-      B = Bt;
-      bufsz = bz;
-      smem = sm;
-    }
+  const int n = g.K0;
+  int B = x_lines_per_cta(F, n, nl);
+  int bufsz = n * (B + 1);
+  size_t smem = (size_t)(n + 2 * (size_t)bufsz) * sizeof(float2);
+  while (smem > 200 * 1024 && B > 8) {
+    B >>= 1;
+    bufsz = n * (B + 1);
+    smem = (size_t)(n + 2 * (size_t)bufsz) * sizeof(float2);
   }
   nblocks = (int)((nl + B - 1) / B);
   fft_x_kernel<MODE><<<nblocks, 256, smem, st>>>(F.len[0], g, inf, iB0, iB1, iB2, cplx, B, bufsz, partials,
-                                                 FastDiv(B));
+                                                 FastDiv(B), FastDiv(B / 8));
   return 1;
 }
 

@@ -14,29 +14,63 @@ namespace spme {
 
 constexpr int kCellWords = 16;  // 9 used: sum_a s_a,i (dE/dr_a)_j
 
+// Cell-sorted view of the points (from the cell sort of the same solve):
+// sorted rank r is point perm[r], in cell key[r] with in-cell fractions
+// rec[r].xyz.  Consecutive threads then read neighbouring grid points.
+struct SortedView {
+  const uint32_t *perm, *key;
+  const float4 *rec;
+  FastDiv K2d, K12d;  // division by K2 and by K1*K2
+};
+
 // CELL: also the per-block sums of s_i (dE/dr)_j over the block's points
 // (s = iL^T x, unwrapped), written to cellp[block][9] in a fixed order.
-template <int P, bool GRAD, bool POT, bool CELL>
+// SORTED: thread r handles point perm[r], with the stencil origin from its
+// cell (k1 = n + 1, argument 1 - f; for f = 0 this is the reference's
+// origin shifted by one cell, whose extra weight M(0) = 0 -- the same sum);
+// otherwise the origin comes from x in FP64 exactly as de2/potl compute it.
+template <int P, bool GRAD, bool POT, bool CELL, bool SORTED>
 __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, const double *__restrict__ x,
                                                      const double *__restrict__ w,
                                                      const float *__restrict__ grid, double *__restrict__ dx,
-                                                     double *__restrict__ phi, double *__restrict__ cellp) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+                                                     double *__restrict__ phi, double *__restrict__ cellp,
+                                                     SortedView sv) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double cacc[9];
   if (CELL) {
 #pragma unroll
     for (int c = 0; c < 9; c++) cacc[c] = 0.0;
   }
-  if (a < n) {
+  if (r < n) {
     const CellConst cc = *g.cell;
-    const double x0 = x[3 * a + 0], x1 = x[3 * a + 1], x2 = x[3 * a + 2];
-    double s0, s1, s2;
-    frac_coords(cc, x0, x1, x2, s0, s1, s2);
-    const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
-                 u2 = __dmul_rn(s2, (double)g.K2);
-    const int c0 = (int)ceil(u0), c1 = (int)ceil(u1), c2 = (int)ceil(u2);
-    const float t0 = (float)((double)c0 - u0), t1 = (float)((double)c1 - u1), t2 = (float)((double)c2 - u2);
-    const int o0 = imod(c0 - P / 2, g.K0), o1 = imod(c1 - P / 2, g.K1), o2 = imod(c2 - P / 2, g.K2);
+    int a, o0, o1, o2;
+    float t0, t1, t2;
+    if (SORTED) {
+      a = (int)sv.perm[r];
+      const uint32_t key = sv.key[r];
+      const float4 u = sv.rec[r];
+      const uint32_t n0 = sv.K12d.div(key), rem = key - n0 * (uint32_t)(g.K1 * g.K2);
+      const uint32_t n1 = sv.K2d.div(rem), n2 = rem - n1 * (uint32_t)g.K2;
+      o0 = imod((int)n0 + 1 - P / 2, g.K0);
+      o1 = imod((int)n1 + 1 - P / 2, g.K1);
+      o2 = imod((int)n2 + 1 - P / 2, g.K2);
+      t0 = 1.f - u.x;
+      t1 = 1.f - u.y;
+      t2 = 1.f - u.z;
+    } else {
+      a = r;
+      double s0, s1, s2;
+      frac_coords(cc, x[3 * a + 0], x[3 * a + 1], x[3 * a + 2], s0, s1, s2);
+      const double u0 = __dmul_rn(s0, (double)g.K0), u1 = __dmul_rn(s1, (double)g.K1),
+                   u2 = __dmul_rn(s2, (double)g.K2);
+      const int c0 = (int)ceil(u0), c1 = (int)ceil(u1), c2 = (int)ceil(u2);
+      t0 = (float)((double)c0 - u0);
+      t1 = (float)((double)c1 - u1);
+      t2 = (float)((double)c2 - u2);
+      o0 = imod(c0 - P / 2, g.K0);
+      o1 = imod(c1 - P / 2, g.K1);
+      o2 = imod(c2 - P / 2, g.K2);
+    }
     float wx[P], dwx[P], wy[P], dwy[P], wz[P], dwz[P];
     int iz[P];
 #pragma unroll
@@ -80,6 +114,7 @@ __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, co
       dx[3 * a + 1] = d1;
       dx[3 * a + 2] = d2;
       if (CELL) {
+        const double x0 = x[3 * a + 0], x1 = x[3 * a + 1], x2 = x[3 * a + 2];
         const double v0 = x0 * cc.iL00 + x1 * cc.iL10 + x2 * cc.iL20;  // unwrapped s
         const double v1 = x1 * cc.iL11 + x2 * cc.iL21;
         const double v2 = x2 * cc.iL22;
@@ -124,44 +159,56 @@ __global__ void cell_grad_kernel(Geom g, const double *__restrict__ cellp, int n
   dEdL[5] = D[2][1];
 }
 
-template <int P>
+template <int P, bool SORTED>
 static int gather_p(const Geom &g, const Spline &S, int n, const double *x, const double *w, const float *grid,
-                    double *dx, double *phi, double *cellp, cudaStream_t st) {
+                    double *dx, double *phi, double *cellp, const SortedView &sv, cudaStream_t st) {
   const int blocks = (n + 255) / 256;
-  if (cellp) gather_kernel<P, true, true, true><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, cellp);
-  else if (dx && phi) gather_kernel<P, true, true, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
-  else if (dx) gather_kernel<P, true, false, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
-  else if (phi) gather_kernel<P, false, true, false><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr);
+  if (cellp)
+    gather_kernel<P, true, true, true, SORTED><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, cellp, sv);
+  else if (dx && phi)
+    gather_kernel<P, true, true, false, SORTED><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr, sv);
+  else if (dx)
+    gather_kernel<P, true, false, false, SORTED><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr, sv);
+  else if (phi)
+    gather_kernel<P, false, true, false, SORTED><<<blocks, 256, 0, st>>>(g, S, n, x, w, grid, dx, phi, nullptr, sv);
   else return 0;
   return 1;
 }
 
-int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,
-                  const float *grid, double *dx, double *phi, cudaStream_t st) {
-  if (n <= 0) return 0;
+template <bool SORTED>
+static int gather_any(const Geom &g, const Spline &S, int n, const double *x, const double *w, const float *grid,
+                      double *dx, double *phi, double *cellp, const SortedView &sv, cudaStream_t st) {
   switch (g.order) {
-    case 2: return gather_p<2>(g, S, n, x, w, grid, dx, phi, nullptr, st);
-    case 4: return gather_p<4>(g, S, n, x, w, grid, dx, phi, nullptr, st);
-    case 6: return gather_p<6>(g, S, n, x, w, grid, dx, phi, nullptr, st);
-    case 8: return gather_p<8>(g, S, n, x, w, grid, dx, phi, nullptr, st);
+    case 2: return gather_p<2, SORTED>(g, S, n, x, w, grid, dx, phi, cellp, sv, st);
+    case 4: return gather_p<4, SORTED>(g, S, n, x, w, grid, dx, phi, cellp, sv, st);
+    case 6: return gather_p<6, SORTED>(g, S, n, x, w, grid, dx, phi, cellp, sv, st);
+    case 8: return gather_p<8, SORTED>(g, S, n, x, w, grid, dx, phi, cellp, sv, st);
     default: return 0;
   }
+}
+
+static SortedView make_view(const Geom &g, const uint32_t *perm, const uint32_t *keys, const float4 *rec) {
+  SortedView sv{perm, keys, rec, FastDiv((uint32_t)g.K2), FastDiv((uint32_t)g.K1 * (uint32_t)g.K2)};
+  return sv;
+}
+
+int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,
+                  const float *grid, double *dx, double *phi, cudaStream_t st, const uint32_t *perm,
+                  const uint32_t *keys, const float4 *rec) {
+  if (n <= 0) return 0;
+  if (perm) return gather_any<true>(g, S, n, x, w, grid, dx, phi, nullptr, make_view(g, perm, keys, rec), st);
+  return gather_any<false>(g, S, n, x, w, grid, dx, phi, nullptr, SortedView{}, st);
 }
 
 // Gather of dE/dx and phi (phi may be null) plus dE/dL; ev must already hold
 // the energy and virial of this solve.  cellp: ceil(n/256) x kCellWords.
 int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, const double *w,
                        const float *grid, double *dx, double *phi, double *cellp, const double *ev, double *dEdL,
-                       cudaStream_t st) {
+                       cudaStream_t st, const uint32_t *perm, const uint32_t *keys, const float4 *rec) {
   int k = 0;
   if (n > 0) {
-    switch (g.order) {
-      case 2: k = gather_p<2>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
-      case 4: k = gather_p<4>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
-      case 6: k = gather_p<6>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
-      case 8: k = gather_p<8>(g, S, n, x, w, grid, dx, phi, cellp, st); break;
-      default: return 0;
-    }
+    if (perm) k = gather_any<true>(g, S, n, x, w, grid, dx, phi, cellp, make_view(g, perm, keys, rec), st);
+    else k = gather_any<false>(g, S, n, x, w, grid, dx, phi, cellp, SortedView{}, st);
   }
   cell_grad_kernel<<<1, 9 * 32, 0, st>>>(g, cellp, (n + 255) / 256, ev, dEdL);
   return k + 1;

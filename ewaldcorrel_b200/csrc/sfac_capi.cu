@@ -581,10 +581,13 @@ static int enqueue_solve(Handle *h, int n, const double *x, const double *w, dou
   if (timed) CK(h, cudaEventRecord(h->ev_stage[4], st));
   k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->d_cell, h->d_red, ev, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[5], st));
+  // gather in cell order (the sort of this solve): neighbouring threads share grid lines
+  const uint32_t *perm = h->sb.vals[h->sb.cur], *skeys = h->sb.keys[h->sb.cur];
   if (dEdL)
-    k += launch_gather_cell(h->geom, h->spline, n, x, w, h->d_real, dx, phi, h->d_cellp, ev, dEdL, st);
+    k += launch_gather_cell(h->geom, h->spline, n, x, w, h->d_real, dx, phi, h->d_cellp, ev, dEdL, st, perm, skeys,
+                            h->sb.rec_sorted);
   else if (n > 0 && (dx || phi))
-    k += launch_gather(h->geom, h->spline, n, x, w, h->d_real, dx, phi, st);
+    k += launch_gather(h->geom, h->spline, n, x, w, h->d_real, dx, phi, st, perm, skeys, h->sb.rec_sorted);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[6], st));
   return k;
 }

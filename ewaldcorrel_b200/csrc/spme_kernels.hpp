@@ -120,13 +120,17 @@ int launch_finish(const double *partials, int nblocks, const CellConst *cell, do
                   cudaStream_t st);
 
 // ---- gather (k_gather.cu) ----
+// perm/keys/rec (optional): the cell-sorted view of the same points (from
+// launch_cell_sort) -- points are then gathered in cell order.
 int launch_gather(const Geom &g, const Spline &S, int n, const double *x, const double *w,
-                  const float *grid, double *dx, double *phi, cudaStream_t st);
+                  const float *grid, double *dx, double *phi, cudaStream_t st, const uint32_t *perm = nullptr,
+                  const uint32_t *keys = nullptr, const float4 *rec = nullptr);
 // Gather + cell adjoint: dE/dL (6 doubles, device) from dE/dx, the virial in ev
 // and the positions; cellp is scratch of gather_cell_words(n) doubles.
 int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, const double *w,
                        const float *grid, double *dx, double *phi, double *cellp, const double *ev, double *dEdL,
-                       cudaStream_t st);
+                       cudaStream_t st, const uint32_t *perm = nullptr, const uint32_t *keys = nullptr,
+                       const float4 *rec = nullptr);
 size_t gather_cell_words(int cap);
 
 }  // namespace spme
