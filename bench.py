@@ -427,6 +427,40 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """`--profile-solves S`: S plain solves (no CUDA graph, no L2 flush, no
+    torch kernels), for profiler captures.  Prints the library's set-up
+    launch count and launches per solve, so a capture can skip the set-up and
+    the first solve (`-s`) and take exactly one solve (`-c`)."""
+    import torch
+
+    from ewaldcorrel_b200 import configs
+    from ewaldcorrel_b200.device import SpmeSolver
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    c = configs.cfg2_water() if args.workload == "water" else configs.cfg3_triclinic()
+    stream = torch.cuda.Stream(dev)
+    solver = SpmeSolver(c.L, c.K, c.order, c.beta, c.max_m, device=0, stream=stream)
+    solver.lib.sfac_set_graphs(solver.handle, 0)
+    x = torch.from_numpy(c.x).to(dev)
+    q = torch.from_numpy(c.q).to(dev)
+    dx = torch.empty((c.n, 3), dtype=torch.float64, device=dev)
+    phi = torch.empty(c.n, dtype=torch.float64, device=dev)
+    ev = torch.empty(7, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    setup = solver.launches()
+    per = []
+    for _ in range(args.profile_solves):
+        l0 = solver.launches()
+        with torch.cuda.stream(stream):
+            solver.solve(x, q, dx, phi, ev)
+        torch.cuda.synchronize(dev)
+        per.append(solver.launches() - l0)
+    print(json.dumps({"profile": args.workload, "setup_launches": setup, "launches_per_solve": per,
+                      "energy": float(ev[0].item())}), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -435,7 +469,12 @@ def main(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS))
+    ap.add_argument("--profile-solves", type=int, default=0,
+                    help="run this many plain solves for a profiler capture and exit (no timing line)")
     args = ap.parse_args(argv)
+    if args.profile_solves > 0:
+        run_profile(args)
+        return
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     local_rank = _env_int("LOCAL_RANK", 0)

@@ -155,6 +155,58 @@ __device__ __forceinline__ void mode_influence(const Influence &inf, const InfCo
   }
 }
 
+// Same A as mode_influence; instead of returning dA it adds sq * A to acc[0]
+// and sq * dA[c] to acc[1 + c] image by image (fewer live registers).
+__device__ __forceinline__ double mode_influence_acc(const Influence &inf, const InfConst &ic, const Geom &g, long i,
+                                                     int kx, int ky, int kz, bool plane, double sq, double (&acc)[7]) {
+  const double wA = plane ? 0.5 : 1.0;
+  if (inf.mode == 1) {
+    const double A = inf.A[i];
+    acc[0] += sq * A;
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[1 + c] += sq * inf.dA[6 * i + c];
+    return A;
+  }
+  const RowImg &r = inf.rows[(long)kx * g.K1 + ky];
+  if (r.count < 0) {
+    double sf, sd[6];
+    ewald_images(ic, g.K0, g.K1, g.K2, kx, ky, kz, sf, sd);
+    const double A = wA * sf;
+    acc[0] += sq * A;
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[1 + c] += sq * (2.0 * wA * sd[c]);
+    return A;
+  }
+  const double fac = -__dmul_rn(3.14159265358979323846 / ic.beta, 3.14159265358979323846 / ic.beta);
+  const double w2 = 2.0 * wA * sq;
+  double sf = 0.0;
+  const int n = r.count;
+  for (int c = 0; c < n; c++) {
+    const int k0 = r.k0[c], k1 = r.k1[c];
+    const int d = kz - k0;
+    int k = k0 + (d >= 0 ? d - (int)inf.K2d.div((uint32_t)d) * g.K2
+                         : (g.K2 - 1) - (int)((uint32_t)(-d - 1) - inf.K2d.div((uint32_t)(-d - 1)) * g.K2));
+    if (k > k1) continue;
+    const double mx = r.mx[c], my = r.my[c], m21 = r.m21[c], mz0 = r.mz0[c];
+    for (; k <= k1; k += g.K2) {
+      const double mz = __dadd_rn(mz0, __dmul_rn((double)k, ic.iL22));
+      const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
+      double fp;
+      sf += ewald_f(m2, fac, fp);
+      const double t = w2 * fp;
+      acc[1] += t * mx * mx;
+      acc[2] += t * my * my;
+      acc[3] += t * mz * mz;
+      acc[4] += t * my * mx;
+      acc[5] += t * mz * mx;
+      acc[6] += t * mz * my;
+    }
+  }
+  const double A = wA * sf;
+  acc[0] += sq * A;
+  return A;
+}
+
 __device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*red)[7], double *out_global) {
   block_reduce_n<7>(acc, red, out_global);
 }

@@ -11,6 +11,7 @@
 // and stores the lines back.  Twiddles come from an FP32 table built in FP64
 // (fft_twiddle_kernel).
 #include "fft_engine.cuh"
+#include "fft_reg.cuh"
 #include "influence.cuh"
 
 namespace spme {
@@ -357,6 +358,145 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
   }
 }
 
+// --- x pass, two-level register transform ---------------------------------
+// Same modes and results as fft_x_kernel, for K0 = n1 * n2 with n1, n2 <= 16.
+// B lines per CTA (a power of two, lines b fastest in the thread index so
+// that every global access is B consecutive complex values); thread t*B + b
+// runs step-1 task j2 = t (t < n2) and step-2 task k1 = t (t < n1) of line b.
+// The exchange buffer holds element (k1, j2) of line b at (k1*n2 + j2)*B + b.
+// The reciprocal step happens on the step-2 registers (all kx = k1 + n1*k2
+// of the line), so forward transform, convolution and inverse transform cost
+// two exchanges in total.
+template <int MODE>
+__global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, const float2 *__restrict__ twg, Geom g,
+                                                     Influence inf, const double *__restrict__ iB0,
+                                                     const double *__restrict__ iB1, const double *__restrict__ iB2,
+                                                     float2 *__restrict__ data, int lgB,
+                                                     double *__restrict__ partials) {
+  extern __shared__ float2 sm[];
+  __shared__ double red[16][7];
+  const int B = 1 << lgB;
+  float2 *tw = sm, *ex = sm + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+  const int ldim = g.ldim, K1 = g.K1;
+  const long nlines = (long)K1 * ldim;
+  const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
+  const long line = (long)blockIdx.x * B + b;
+  const bool live = line < nlines;
+  const int ky = live ? (int)(line / ldim) : 0, kz = live ? (int)(line - (long)ky * ldim) : 0;
+  constexpr bool FWD = (MODE == XM_FWD_DECONV || MODE == XM_FWD_CONV_INV);
+  __syncthreads();
+  if (FWD && t < n2) {
+    const int j2 = t;
+    rdft::with_radix(n1, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 u[R];
+#pragma unroll
+      for (int j1 = 0; j1 < R; j1++)
+        u[j1] = live ? data[line + (long)(j2 + n2 * j1) * nlines] : make_float2(0.f, 0.f);
+      rdft::dft<R, -1>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], tw[j2 * k1]);
+    });
+  }
+  if (FWD) __syncthreads();
+  double acc[7];
+#pragma unroll
+  for (int c = 0; c < 7; c++) acc[c] = 0.0;
+  if (t < n1) {
+    const int k1 = t;
+    rdft::with_radix(n2, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 w[R];
+      if (FWD) {
+#pragma unroll
+        for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
+        rdft::dft<R, -1>(w);
+      } else {
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++)
+          w[k2] = live ? data[line + (long)(k1 + n1 * k2) * nlines] : make_float2(0.f, 0.f);
+      }
+      if (MODE == XM_FWD_DECONV) {
+        if (live) {
+          const double s12 = iB1[ky] * iB2[kz];
+#pragma unroll
+          for (int k2 = 0; k2 < R; k2++) {
+            const int kx = k1 + n1 * k2;
+            data[line + (long)kx * nlines] = cscale(w[k2], (float)(iB0[kx] * s12));
+          }
+        }
+      } else {
+        // the pointwise step walks the line's values through the thread's
+        // own exchange slots (a run-time index into registers would spill)
+        float2 *slot = ex + k1 * n2 * B + b;
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++) slot[k2 * B] = w[k2];
+        if (live) {
+          const bool even = (g.K2 % 2) == 0;
+          const bool plane = (kz == 0) || (even && kz == ldim - 1);
+          const InfConst ic = load_ic(inf);
+          const double s12 = iB1[ky] * iB2[kz];
+#pragma unroll 1
+          for (int k2 = 0; k2 < R; k2++) {
+            const int kx = k1 + n1 * k2;
+            const long i = ((long)kx * K1 + ky) * ldim + kz;
+            const float2 q = slot[k2 * B];
+            const double ib = iB0[kx] * s12;
+            double sq = (double)q.x * q.x + (double)q.y * q.y;
+            if (MODE == XM_FWD_CONV_INV) sq *= ib * ib;  // |F iB|^2
+            const double A = mode_influence_acc(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
+            if (MODE != XM_EN) {
+              double f = A * ib * (MODE == XM_FWD_CONV_INV ? ib : 1.0);
+              if (plane) f *= 2.0;
+              slot[k2 * B] = cscale(q, (float)f);
+            }
+          }
+        }
+        if (MODE != XM_EN) {
+#pragma unroll
+          for (int k2 = 0; k2 < R; k2++) w[k2] = slot[k2 * B];
+          rdft::dft<R, +1>(w);
+#pragma unroll
+          for (int j2 = 0; j2 < R; j2++) {
+            float2 c = tw[j2 * k1];
+            c.y = -c.y;
+            ex[(k1 * n2 + j2) * B + b] = cmul(w[j2], c);
+          }
+        }
+      }
+    });
+  }
+  if (MODE != XM_FWD_DECONV) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 7; c++) {
+      const double v = warp_sum(acc[c]);
+      if (lane == 0) red[warp][c] = v;
+    }
+  }
+  if (MODE == XM_FWD_DECONV) return;
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w][threadIdx.x];
+    partials[(long)blockIdx.x * kRedWords + threadIdx.x] = v;
+  }
+  if (MODE == XM_EN) return;
+  if (t < n2 && live) {
+    const int j2 = t;
+    rdft::with_radix(n1, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 u[R];
+#pragma unroll
+      for (int k1 = 0; k1 < R; k1++) u[k1] = ex[(k1 * n2 + j2) * B + b];
+      rdft::dft<R, +1>(u);
+#pragma unroll
+      for (int j1 = 0; j1 < R; j1++) data[line + (long)(j2 + n2 * j1) * nlines] = u[j1];
+    });
+  }
+}
+
 // FP32 twiddles exp(-2 pi i k / n), evaluated in FP64.
 __global__ void fft_twiddle_kernel(int n, float2 *tw) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -412,6 +552,11 @@ void fft_prepare_kernels() {
   cudaFuncSetAttribute((const void *)fft_x_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        lim);
   cudaFuncSetAttribute((const void *)fft_x_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_FWD_DECONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       lim);
+  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 // Shared memory of the plane kernels: twiddles + two buffers of `sz`.
@@ -502,11 +647,43 @@ static int x_lines_per_cta(const FftPlan3 &F, int n, long nlines) {
   return B;
 }
 
+// Two-level x pass: lines per CTA B = 2^lgB (8..32) with B*max(n1, n2)
+// threads (<= 512), halved while fewer than two CTAs per SM would run;
+// x_lines overrides B.  Returns false when K0 has no n1 * n2 split.
+static bool x2_shape(const FftPlan3 &F, int n, long nlines, int &n1, int &n2, int &lgB, int &threads) {
+  if (!rdft::split_line(n, n1, n2)) return false;
+  const int m = n1 > n2 ? n1 : n2;
+  int B;
+  if (F.x_lines > 0) {
+    B = 8;
+    while (B < F.x_lines && B < 32) B <<= 1;
+  } else {
+    B = 8;
+    while (B < 32 && B * m < 128) B <<= 1;
+    while (B > 8 && (nlines + B - 1) / B < 2 * 148) B >>= 1;
+  }
+  while (B > 8 && B * m > 512) B >>= 1;
+  if (B * m > 512) return false;
+  lgB = 0;
+  while ((1 << lgB) < B) lgB++;
+  threads = (B * m + 31) / 32 * 32;
+  return true;
+}
+
 template <int MODE>
 static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, int &nblocks, cudaStream_t st) {
   const long nl = (long)g.K1 * g.ldim;
   const int n = g.K0;
+  int n1, n2, lgB, threads;
+  if (x2_shape(F, n, nl, n1, n2, lgB, threads)) {
+    const int B = 1 << lgB;
+    const size_t smem = (size_t)(n + (size_t)B * n) * sizeof(float2);
+    nblocks = (int)((nl + B - 1) / B);
+    fft_x2_kernel<MODE><<<nblocks, threads, smem, st>>>(n, n1, n2, F.len[0].tw, g, inf, iB0, iB1, iB2, cplx, lgB,
+                                                        partials);
+    return 1;
+  }
   int B = x_lines_per_cta(F, n, nl);
   int bufsz = n * (B + 1);
   size_t smem = (size_t)(n + 2 * (size_t)bufsz) * sizeof(float2);

@@ -187,22 +187,32 @@ __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
   }
 }
 
-// cell_start[c] = first sorted rank whose key >= c, for c in [0, ncell]; one
-// thread per run of 32 cells (binary search, then a forward walk).
-constexpr int CS_RUN = 32;
+// cell_start[c] = first sorted rank whose key >= c, for c in [0, ncell].
+// With k(i) the sorted keys, k(-1) = -1 and k(n) = ncell, rank i is the
+// answer for exactly the cells (k(i-1), k(i)].  One warp takes 32 ranks:
+// it walks the contiguous cell range (k(i0-1), k(i0+31)] in chunks of 32
+// cells, each lane finding its cell's rank among the warp's 32 keys by a
+// register binary search (shuffles), so every store is coalesced and no
+// global search is needed.  Work: (n + ncell) / 32 warp steps.
 __global__ void __launch_bounds__(256) cell_start_kernel(int n, const uint32_t *__restrict__ keys, long ncell,
                                                          int *__restrict__ cell_start) {
-  const long c0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * CS_RUN;
-  if (c0 > ncell) return;
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if ((long)keys[mid] < c0) lo = mid + 1; else hi = mid;
-  }
-  const long c1 = min(c0 + CS_RUN, ncell + 1);
-  for (long c = c0; c < c1; c++) {
-    while (lo < n && (long)keys[lo] < c) lo++;
-    cell_start[c] = lo;
+  const long i0 = (((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+  const int lane = threadIdx.x & 31;
+  if (i0 > n) return;  // warp-uniform
+  const long i = i0 + lane;
+  const long kl = (i < n) ? (long)keys[i] : ncell;  // ranks beyond n: empty ranges at ncell
+  const long prev = (i0 == 0) ? -1 : (long)keys[i0 - 1];
+  const long last = __shfl_sync(0xffffffffu, kl, 31);
+  for (long cb = prev + 1; cb <= last; cb += 32) {
+    const long c = cb + lane;
+    // smallest l with k(i0 + l) >= c (exists for c <= last)
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+      const long kv = __shfl_sync(0xffffffffu, kl, l + step - 1);
+      if (kv < c) l += step;
+    }
+    if (c <= last) cell_start[c] = (int)(i0 + l);
   }
 }
 
@@ -249,8 +259,8 @@ int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, Sor
     }
     b.cur = src;
   }
-  cell_start_kernel<<<ceil_div(ceil_div(ncell + 1, CS_RUN), 256), 256, 0, st>>>(n, b.keys[b.cur], ncell,
-                                                                                   b.cell_start);
+  cell_start_kernel<<<ceil_div(ceil_div((long)n + 1, 32) * 32, 256), 256, 0, st>>>(n, b.keys[b.cur], ncell,
+                                                                                      b.cell_start);
   return launches + 1;
 }
 

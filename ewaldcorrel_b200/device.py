@@ -31,6 +31,8 @@ def _lib():
         lib.sfac_solve_device.restype = c_int
         lib.sfac_solve_device_timed.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [ctypes.POINTER(c_float)]
         lib.sfac_solve_device_timed.restype = c_int
+        lib.sfac_set_graphs.argtypes = [c_void_p, c_int]
+        lib.sfac_set_graphs.restype = c_int
         lib._device_declared = True
     return lib
 
