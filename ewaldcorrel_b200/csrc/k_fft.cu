@@ -497,6 +497,185 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
   }
 }
 
+// --- per-axis passes, two-level register transform -------------------------
+// Thread t*B + b works on line b of the CTA's B (= 2^lgB) lines: step-1 task
+// j2 = t (t < n2), step-2 task k1 = t (t < n1); exchange slot of element
+// (k1, j2) of line b: (k1*n2 + j2)*B + b.  tw: exp(-2 pi i e / n), e < n.
+
+// y pass: complex lines along y of every x-plane; line l = x*lpp + kz at
+// data[x*pstride + kz + j*es].  With `partials`, CTA 0 first reduces the
+// preceding x pass's energy/virial partials (needs >= 7 warps).
+template <int SIGN>
+__global__ void __launch_bounds__(512) fft_y2_kernel(int n, int n1, int n2, const float2 *__restrict__ twg,
+                                                     float2 *__restrict__ data, long nlines, FastDiv lpp,
+                                                     long pstride, int es, int lgB,
+                                                     const double *__restrict__ partials, int nblocks,
+                                                     const CellConst *__restrict__ cell, double *__restrict__ raw,
+                                                     double *__restrict__ ev) {
+  if (partials && blockIdx.x == 0) finish_partials(partials, nblocks, cell, raw, ev);
+  extern __shared__ float2 sm[];
+  const int B = 1 << lgB;
+  float2 *tw = sm, *ex = sm + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+  const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
+  const long l = (long)blockIdx.x * B + b;
+  const bool live = l < nlines;
+  uint32_t pl = 0, r = 0;
+  if (live) lpp.divmod((uint32_t)l, pl, r);
+  const long base = (long)pl * pstride + r;
+  __syncthreads();
+  if (t < n2) {
+    const int j2 = t;
+    rdft::with_radix(n1, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 u[R];
+#pragma unroll
+      for (int j1 = 0; j1 < R; j1++) u[j1] = live ? data[base + (long)(j2 + n2 * j1) * es] : make_float2(0.f, 0.f);
+      rdft::dft<R, SIGN>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], twid<SIGN>(tw, j2 * k1));
+    });
+  }
+  __syncthreads();
+  if (t < n1 && live) {
+    const int k1 = t;
+    rdft::with_radix(n2, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 w[R];
+#pragma unroll
+      for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
+      rdft::dft<R, SIGN>(w);
+#pragma unroll
+      for (int k2 = 0; k2 < R; k2++) data[base + (long)(k1 + n1 * k2) * es] = w[k2];
+    });
+  }
+}
+
+// z pass, real to half-complex: 2B consecutive real rows of length n per
+// CTA (row pair b forms the complex line row[2b] + i row[2b+1]); the rows
+// are read and the ldim = n/2 + 1 outputs written as contiguous blocks.
+// Shared: tw[n] | ex[B*n] | rows (2B x (n+1) floats), later Z (B x (n+1) complex).
+__global__ void __launch_bounds__(512) fft_zr2c2_kernel(int n, int n1, int n2, const float2 *__restrict__ twg,
+                                                        const float *__restrict__ rin, float2 *__restrict__ cout,
+                                                        long nrows, int lgB) {
+  extern __shared__ float2 sm[];
+  const int B = 1 << lgB, ldim = n / 2 + 1, RP = n + 1, ZP = n + 1;
+  float2 *tw = sm, *ex = sm + n, *Z = ex + B * n;
+  float *rows = reinterpret_cast<float *>(Z);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+  const long row0 = (long)blockIdx.x * 2 * B;
+  const int nr = (int)min((long)(2 * B), nrows - row0);
+  const float *src = rin + row0 * n;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
+    for (int j = lane; j < n; j += 32) rows[rr * RP + j] = (rr < nr) ? src[(long)rr * n + j] : 0.f;
+  __syncthreads();
+  const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
+  if (t < n2) {
+    const int j2 = t;
+    const float *ra = rows + (2 * b) * RP, *rb = ra + RP;
+    rdft::with_radix(n1, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 u[R];
+#pragma unroll
+      for (int j1 = 0; j1 < R; j1++) u[j1] = make_float2(ra[j2 + n2 * j1], rb[j2 + n2 * j1]);
+      rdft::dft<R, -1>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], tw[j2 * k1]);
+    });
+  }
+  __syncthreads();
+  if (t < n1) {
+    const int k1 = t;
+    rdft::with_radix(n2, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 w[R];
+#pragma unroll
+      for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
+      rdft::dft<R, -1>(w);
+#pragma unroll
+      for (int k2 = 0; k2 < R; k2++) Z[b * ZP + k1 + n1 * k2] = w[k2];
+    });
+  }
+  __syncthreads();
+  float2 *dst = cout + row0 * ldim;
+  for (int rr = threadIdx.x >> 5; rr < nr; rr += nw) {
+    const float2 *zb = Z + (rr >> 1) * ZP;
+    for (int k = lane; k < ldim; k += 32) {
+      const float2 u = zb[k], v = zb[k == 0 ? 0 : n - k];
+      dst[(long)rr * ldim + k] = (rr & 1) ? make_float2(0.5f * (u.y + v.y), -0.5f * (u.x - v.x))
+                                          : make_float2(0.5f * (u.x + v.x), 0.5f * (u.y - v.y));
+    }
+  }
+}
+
+// z pass, half-complex to real: the inverse of fft_zr2c2_kernel.  The
+// complex line of row pair b is X_2b + i X_2b+1 over the full length (the
+// Hermitian extension; self-conjugate bins keep their real parts only, as a
+// c2r transform ignores their imaginary parts).
+// Shared: tw[n] | ex[B*n] | H (2B x (ldim+1) complex), later rows (2B x (n+1) floats).
+__global__ void __launch_bounds__(512) fft_zc2r2_kernel(int n, int n1, int n2, const float2 *__restrict__ twg,
+                                                        const float2 *__restrict__ cin, float *__restrict__ rout,
+                                                        long nrows, int lgB) {
+  extern __shared__ float2 sm[];
+  const int B = 1 << lgB, ldim = n / 2 + 1, HP = ldim + 1, RP = n + 1;
+  float2 *tw = sm, *ex = sm + n, *H = ex + B * n;
+  float *rows = reinterpret_cast<float *>(H);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = twg[i];
+  const long row0 = (long)blockIdx.x * 2 * B;
+  const int nr = (int)min((long)(2 * B), nrows - row0);
+  const float2 *src = cin + row0 * ldim;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
+    for (int k = lane; k < ldim; k += 32) H[rr * HP + k] = (rr < nr) ? src[(long)rr * ldim + k] : make_float2(0.f, 0.f);
+  __syncthreads();
+  const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
+  if (t < n2) {
+    const int j2 = t;
+    const float2 *ha = H + (2 * b) * HP, *hb = ha + HP;
+    rdft::with_radix(n1, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 u[R];
+#pragma unroll
+      for (int j1 = 0; j1 < R; j1++) {
+        const int k = j2 + n2 * j1;
+        const bool lo = k < ldim;
+        const int kk = lo ? k : n - k;
+        float2 a = ha[kk], c = hb[kk];
+        if (kk == 0 || 2 * kk == n) {
+          a.y = 0.f;
+          c.y = 0.f;
+        }
+        u[j1] = lo ? make_float2(a.x - c.y, a.y + c.x) : make_float2(a.x + c.y, c.x - a.y);
+      }
+      rdft::dft<R, +1>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], twid<+1>(tw, j2 * k1));
+    });
+  }
+  __syncthreads();
+  if (t < n1) {
+    const int k1 = t;
+    float *ra = rows + (2 * b) * RP, *rb = ra + RP;
+    rdft::with_radix(n2, [&](auto RI) {
+      constexpr int R = decltype(RI)::value;
+      float2 w[R];
+#pragma unroll
+      for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
+      rdft::dft<R, +1>(w);
+#pragma unroll
+      for (int k2 = 0; k2 < R; k2++) {
+        ra[k1 + n1 * k2] = w[k2].x;
+        rb[k1 + n1 * k2] = w[k2].y;
+      }
+    });
+  }
+  __syncthreads();
+  float *dst = rout + row0 * n;
+  for (int rr = threadIdx.x >> 5; rr < nr; rr += nw)
+    for (int j = lane; j < n; j += 32) dst[(long)rr * n + j] = rows[rr * RP + j];
+}
+
 // FP32 twiddles exp(-2 pi i k / n), evaluated in FP64.
 __global__ void fft_twiddle_kernel(int n, float2 *tw) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -557,6 +736,10 @@ void fft_prepare_kernels() {
   cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        lim);
   cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_y2_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_y2_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_zr2c2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute((const void *)fft_zc2r2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 // Shared memory of the plane kernels: twiddles + two buffers of `sz`.
@@ -575,25 +758,74 @@ bool fft_plane_fits(int K1, int K2) {
 
 long fft_x_blocks_max(int K1, int K2) { return ((long)K1 * (K2 / 2 + 1) + 7) / 8; }
 
-// Forward z (r2c) and y transforms: one fused plane kernel when an x-plane
-// fits in shared memory, else one pass per axis.
+// Shape of a two-level per-axis pass over `nlines` lines of length n:
+// B = 2^lgB lines per CTA (8..32), B*max(n1, n2) threads (at least
+// min_threads, at most 512), B halved while fewer than two CTAs per SM
+// (148 SMs) would run.  False when n has no n1 * n2 split.
+static bool lines2_shape(int n, long nlines, int min_threads, int &n1, int &n2, int &lgB, int &threads) {
+  if (!rdft::split_line(n, n1, n2)) return false;
+  const int m = n1 > n2 ? n1 : n2;
+  int B = 8;
+  while (B < 32 && B * m < 128) B <<= 1;
+  while (B > 8 && (nlines + B - 1) / B < 2 * 148) B >>= 1;
+  while (B > 8 && B * m > 512) B >>= 1;
+  if (B * m > 512) return false;
+  lgB = 0;
+  while ((1 << lgB) < B) lgB++;
+  threads = (B * m + 31) / 32 * 32;
+  if (threads < min_threads) threads = min_threads;
+  return true;
+}
+
+// Which z/y implementation a plan uses: the fused plane kernels (an x-plane
+// in shared memory), the two-level per-axis passes, or the Stockham
+// per-axis passes (any length).
+enum { ZY_PLANE = 1, ZY_TWO_LEVEL = 2, ZY_STOCKHAM = 3 };
+static int zy_choice(const FftPlan3 &F) {
+  const int K1 = F.len[1].n, K2 = F.len[2].n;
+  int sz, a, b;
+  const bool plane = plane_smem(K1, K2, sz) <= kPlaneSmemMax;
+  const bool two = rdft::split_line(K1, a, b) && rdft::split_line(K2, a, b);
+  if (F.zy_mode == ZY_PLANE && plane) return ZY_PLANE;
+  if (F.zy_mode == ZY_STOCKHAM) return ZY_STOCKHAM;
+  if (two) return ZY_TWO_LEVEL;
+  return plane ? ZY_PLANE : ZY_STOCKHAM;
+}
+
+// Forward z (r2c) and y transforms.
 int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st) {
   const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
-  int sz;
-  const size_t psm = plane_smem(K1, K2, sz);
-  if (psm <= kPlaneSmemMax) {
+  const int zy = zy_choice(F);
+  if (zy == ZY_PLANE) {
+    int sz;
+    const size_t psm = plane_smem(K1, K2, sz);
     const int nb1 = (K1 + 1) / 2;
     fft_plane_fwd_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], real, cplx, sz, FastDiv((nb1 + 15) / 16),
                                                FastDiv((ldim + 15) / 16), FastDiv(K2), FastDiv(ldim));
     return 1;
   }
+  const long nrows = (long)K0 * K1;
+  const long nl = (long)K0 * ldim;
+  if (zy == ZY_TWO_LEVEL) {
+    int n1, n2, lgB, thr;
+    lines2_shape(K2, (nrows + 1) / 2, 0, n1, n2, lgB, thr);
+    int B = 1 << lgB;
+    size_t smem = (size_t)(K2 + (size_t)B * K2 + (size_t)B * (K2 + 4)) * sizeof(float2);
+    fft_zr2c2_kernel<<<(unsigned)((nrows + 2 * B - 1) / (2 * B)), thr, smem, st>>>(K2, n1, n2, F.len[2].tw, real,
+                                                                                  cplx, nrows, lgB);
+    lines2_shape(K1, nl, 0, n1, n2, lgB, thr);
+    B = 1 << lgB;
+    smem = (size_t)(K1 + (size_t)B * K1) * sizeof(float2);
+    fft_y2_kernel<-1><<<(unsigned)((nl + B - 1) / B), thr, smem, st>>>(K1, n1, n2, F.len[1].tw, cplx, nl,
+                                                                       FastDiv(ldim), (long)K1 * ldim, ldim, lgB,
+                                                                       nullptr, 0, nullptr, nullptr, nullptr);
+    return 2;
+  }
   int B, bufsz;
   size_t smem;
-  const int nrows = K0 * K1;
   fft_shape(K2, (nrows + 1) / 2, B, bufsz, smem);
-  fft_z_r2c_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, real, cplx, ldim, B, bufsz,
-                                                                      FastDiv(B));
-  const long nl = (long)K0 * ldim;
+  fft_z_r2c_kernel<<<(unsigned)((nrows + 2 * B - 1) / (2 * B)), 256, smem, st>>>(F.len[2], (int)nrows, real, cplx,
+                                                                                 ldim, B, bufsz, FastDiv(B));
   fft_shape(K1, nl, B, bufsz, smem);
   DeconvArgs none{};
   fft_strided_kernel<-1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim, ldim,
@@ -602,32 +834,48 @@ int fwd_zy(const FftPlan3 &F, const float *real, float2 *cplx, cudaStream_t st) 
 }
 
 // Inverse y and z (c2r) transforms; with `partials`, the energy/virial
-// partials are reduced first (inside the plane kernel when it is used).
+// partials are reduced first (inside the first kernel when it can).
 int inv_yz(const FftPlan3 &F, float2 *cplx, float *real, const double *partials, int nblocks,
            const CellConst *cell, double *raw, double *ev, cudaStream_t st) {
   const int K0 = F.len[0].n, K1 = F.len[1].n, K2 = F.len[2].n, ldim = K2 / 2 + 1;
-  int sz;
-  const size_t psm = plane_smem(K1, K2, sz);
-  if (psm <= kPlaneSmemMax) {
+  const int zy = zy_choice(F);
+  if (zy == ZY_PLANE) {
+    int sz;
+    const size_t psm = plane_smem(K1, K2, sz);
     const int nb1 = (K1 + 1) / 2;
     fft_plane_inv_kernel<<<K0, 512, psm, st>>>(F.len[1], F.len[2], cplx, real, sz, partials, nblocks, cell, raw,
                                                ev, FastDiv((nb1 + 15) / 16), FastDiv((ldim + 15) / 16), FastDiv(K2),
                                                FastDiv(ldim), FastDiv(nb1));
     return 1;
   }
+  const long nrows = (long)K0 * K1;
+  const long nl = (long)K0 * ldim;
+  if (zy == ZY_TWO_LEVEL) {
+    int n1, n2, lgB, thr;
+    lines2_shape(K1, nl, partials ? 256 : 0, n1, n2, lgB, thr);
+    int B = 1 << lgB;
+    size_t smem = (size_t)(K1 + (size_t)B * K1) * sizeof(float2);
+    fft_y2_kernel<+1><<<(unsigned)((nl + B - 1) / B), thr, smem, st>>>(K1, n1, n2, F.len[1].tw, cplx, nl,
+                                                                       FastDiv(ldim), (long)K1 * ldim, ldim, lgB,
+                                                                       partials, nblocks, cell, raw, ev);
+    lines2_shape(K2, (nrows + 1) / 2, 0, n1, n2, lgB, thr);
+    B = 1 << lgB;
+    smem = (size_t)(K2 + (size_t)B * K2 + (size_t)B * (K2 + 4)) * sizeof(float2);
+    fft_zc2r2_kernel<<<(unsigned)((nrows + 2 * B - 1) / (2 * B)), thr, smem, st>>>(K2, n1, n2, F.len[2].tw, cplx,
+                                                                                  real, nrows, lgB);
+    return 2;
+  }
   int k = 0;
   if (partials) k += launch_finish(partials, nblocks, cell, raw, ev, st);
   int B, bufsz;
   size_t smem;
-  const long nl = (long)K0 * ldim;
   fft_shape(K1, nl, B, bufsz, smem);
   DeconvArgs none{};
   fft_strided_kernel<+1><<<(int)((nl + B - 1) / B), 256, smem, st>>>(F.len[1], nl, ldim, (long)K1 * ldim, ldim,
                                                                      cplx, B, bufsz, none, FastDiv(B));
-  const int nrows = K0 * K1;
   fft_shape(K2, (nrows + 1) / 2, B, bufsz, smem);
-  fft_z_c2r_kernel<<<(nrows + 2 * B - 1) / (2 * B), 256, smem, st>>>(F.len[2], nrows, cplx, real, ldim, B, bufsz,
-                                                                      FastDiv(B));
+  fft_z_c2r_kernel<<<(unsigned)((nrows + 2 * B - 1) / (2 * B)), 256, smem, st>>>(F.len[2], (int)nrows, cplx, real,
+                                                                                 ldim, B, bufsz, FastDiv(B));
   return k + 2;
 }
 

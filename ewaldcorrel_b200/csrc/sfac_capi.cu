@@ -281,6 +281,10 @@ void *sfac_ctor(double L[6], int K[3], int order) {
   make_spline(order, h->spline, h->nodes);
   fft_prepare_kernels();
   if (const char *e = getenv("SFAC_NO_GRAPH")) h->use_graph = !(e[0] && e[0] != '0');
+  if (const char *e = getenv("SFAC_ZY_MODE")) {
+    const int v = atoi(e);
+    if (v >= 0 && v <= 3) h->fft.zy_mode = v;
+  }
 
   bool ok = CK(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) &&
             CK(h, cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
@@ -677,6 +681,12 @@ int sfac_set_tuning(void *p, int key, int value) {
   if (key == SFAC_TUNE_X_LINES) {
     if (value < 0 || value > 64 || (value & (value - 1))) return 1;
     h->fft.x_lines = value;
+    h->version++;
+    return 0;
+  }
+  if (key == SFAC_TUNE_ZY_MODE) {
+    if (value < 0 || value > 3) return 1;
+    h->fft.zy_mode = value;
     h->version++;
     return 0;
   }

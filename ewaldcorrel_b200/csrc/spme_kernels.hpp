@@ -39,6 +39,7 @@ struct FftLen {
 struct FftPlan3 {
   FftLen len[3];
   int x_lines = 0;  // lines per CTA of the x pass (0: heuristic); set by the autotuner
+  int zy_mode = 0;  // z/y passes: 0 automatic, 1 fused plane kernels, 2 two-level, 3 Stockham
 };
 struct DeconvArgs {
   const double *iB0, *iB1, *iB2;  // null: no moduli division

@@ -148,8 +148,11 @@ int sfac_set_graphs(void *sfac, int enable);
 
 /* Tuning knobs chosen by an autotuner (0 restores the heuristic):
  * SFAC_TUNE_X_LINES: x-FFT lines per CTA (power of two, <= 64).
+ * SFAC_TUNE_ZY_MODE: z/y FFT passes: 1 fused x-plane kernels (when a plane
+ *   fits in shared memory), 2 two-level register passes, 3 Stockham passes.
  * Returns 0, or 1 for an unknown key or bad value. */
 #define SFAC_TUNE_X_LINES 1
+#define SFAC_TUNE_ZY_MODE 2
 int sfac_set_tuning(void *sfac, int key, int value);
 
 /* Estimated device + pinned-host bytes of a handle with grid K solving n
