@@ -8,14 +8,17 @@
 namespace spme {
 
 // Ewald influence function f(m^2) = exp(-pi^2 m^2 / beta^2) / (pi m^2) and
-// f'(m^2) = (-pi^2/beta^2 - 1/m^2) f  (ewald.py:124-132; f(0) = 0).
+// f'(m^2) = (-pi^2/beta^2 - 1/m^2) f  (ewald.py:124-132; f(0) = 0), with
+// fac = -pi^2/beta^2.  One correctly rounded reciprocal of m^2 serves both.
 __device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
   if (r2 < 1e-10) {
     fp = 0.0;
     return 0.0;
   }
-  const double f = exp(r2 * fac) / (r2 * 3.14159265358979323846);
-  fp = (fac - 1.0 / r2) * f;
+  constexpr double kInvPi = 0.318309886183790671537767526745028724;
+  const double ir2 = __drcp_rn(r2);
+  const double f = exp(r2 * fac) * (ir2 * kInvPi);
+  fp = (fac - ir2) * f;
   return f;
 }
 
@@ -28,7 +31,7 @@ __device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
 __device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1, int K2, int kx, int ky, int kz,
                              double &sf, double sd[6]) {
   const double R2 = __dmul_rn(inf.max_m, inf.max_m);
-  const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
+  const double fac = inf.fac;
   const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
   sf = 0.0;
   for (int c = 0; c < 6; c++) sd[c] = 0.0;
@@ -99,7 +102,7 @@ __device__ __forceinline__ int ewald_row(const InfConst &inf, int K0, int K1, in
 // the z images (k = kz mod K2 within [k0, k1]) and their exp are evaluated.
 __device__ __forceinline__ void ewald_images_row(const InfConst &inf, const FastDiv &K2d, const RowImg &r, int K2,
                                                  int kz, double &sf, double sd[6]) {
-  const double fac = -__dmul_rn(3.14159265358979323846 / inf.beta, 3.14159265358979323846 / inf.beta);
+  const double fac = inf.fac;
   sf = 0.0;
   for (int c = 0; c < 6; c++) sd[c] = 0.0;
   const int n = r.count;
@@ -177,7 +180,7 @@ __device__ __forceinline__ double mode_influence_acc(const Influence &inf, const
     for (int c = 0; c < 6; c++) acc[1 + c] += sq * (2.0 * wA * sd[c]);
     return A;
   }
-  const double fac = -__dmul_rn(3.14159265358979323846 / ic.beta, 3.14159265358979323846 / ic.beta);
+  const double fac = ic.fac;
   const double w2 = 2.0 * wA * sq;
   double sf = 0.0;
   const int n = r.count;

@@ -14,6 +14,57 @@ namespace spme {
 
 constexpr int kCellWords = 16;  // 9 used: sum_a s_a,i (dE/dr_a)_j
 
+// idx[i] = (o + i) mod K for 0 <= o < K, without a division when K >= P.
+template <int P>
+__device__ __forceinline__ void wrap_run(int o, int K, int (&idx)[P]) {
+  if (K >= P) {
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+      const int v = o + i;
+      idx[i] = v >= K ? v - K : v;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < P; i++) idx[i] = (o + i) % K;
+  }
+}
+
+// Order-P stencil sum of the grid around one point, factorised per axis:
+// pot = sum_i wx_i sum_j wy_j sum_k wz_k Q, and the three derivatives.
+// WRAP false: the z indices are z0 .. z0 + P - 1; true: iz[k] (z0 = 0).
+template <int P, bool WRAP>
+__device__ __forceinline__ void stencil_sum(const float *__restrict__ grid, const Geom &g, int o0,
+                                            const int (&iy)[P], int z0, const int (&iz)[P], const float (&wx)[P],
+                                            const float (&dwx)[P], const float (&wy)[P], const float (&dwy)[P],
+                                            const float (&wz)[P], const float (&dwz)[P], float &pot, float &gx,
+                                            float &gy, float &gz) {
+  const long plane = (long)g.K1 * g.K2;
+  int xi = o0;  // (o0 + i) mod K0
+#pragma unroll 1
+  for (int i = 0; i < P; i++, xi = (xi + 1 == g.K0) ? 0 : xi + 1) {
+    const float *pl = grid + xi * plane + z0;
+    float sy = 0.f, dy = 0.f, dz = 0.f;
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+      const float *col = pl + (long)iy[j] * g.K2;
+      float sz = 0.f, dzz = 0.f;
+#pragma unroll
+      for (int k = 0; k < P; k++) {
+        const float q = __ldg(col + (WRAP ? iz[k] : k));
+        sz = fmaf(wz[k], q, sz);
+        dzz = fmaf(dwz[k], q, dzz);
+      }
+      sy = fmaf(wy[j], sz, sy);
+      dy = fmaf(dwy[j], sz, dy);
+      dz = fmaf(wy[j], dzz, dz);
+    }
+    pot = fmaf(wx[i], sy, pot);
+    gx = fmaf(dwx[i], sy, gx);
+    gy = fmaf(wx[i], dy, gy);
+    gz = fmaf(wx[i], dz, gz);
+  }
+}
+
 // Cell-sorted view of the points (from the cell sort of the same solve):
 // sorted rank r is point perm[r], in cell key[r] with in-cell fractions
 // rec[r].xyz.  Consecutive threads then read neighbouring grid points.
@@ -72,37 +123,23 @@ __global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, co
       o2 = imod(c2 - P / 2, g.K2);
     }
     float wx[P], dwx[P], wy[P], dwy[P], wz[P], dwz[P];
-    int iz[P];
 #pragma unroll
     for (int i = 0; i < P; i++) {
       dbspl_eval(S, P, t0, i, wx[i], dwx[i]);
       dbspl_eval(S, P, t1, i, wy[i], dwy[i]);
       dbspl_eval(S, P, t2, i, wz[i], dwz[i]);
-      iz[i] = (o2 + i) % g.K2;
     }
+    int iy[P];
+    wrap_run<P>(o1, g.K1, iy);
     float pot = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll 1
-    for (int i = 0; i < P; i++) {
-      const long row_x = (long)((o0 + i) % g.K0) * g.K1;
-      float sy = 0.f, dy = 0.f, dz = 0.f;
-#pragma unroll
-      for (int j = 0; j < P; j++) {
-        const float *col = grid + (row_x + (o1 + j) % g.K1) * g.K2;
-        float sz = 0.f, dzz = 0.f;
-#pragma unroll
-        for (int k = 0; k < P; k++) {
-          const float q = __ldg(col + iz[k]);
-          sz = fmaf(wz[k], q, sz);
-          dzz = fmaf(dwz[k], q, dzz);
-        }
-        sy = fmaf(wy[j], sz, sy);
-        dy = fmaf(dwy[j], sz, dy);
-        dz = fmaf(wy[j], dzz, dz);
-      }
-      pot = fmaf(wx[i], sy, pot);
-      gx = fmaf(dwx[i], sy, gx);
-      gy = fmaf(wx[i], dy, gy);
-      gz = fmaf(wx[i], dz, gz);
+    int iz[P];
+    // Warp-uniform choice (no divergent second copy of the stencil): when no
+    // active lane's z run wraps, constant offsets from one address per row.
+    if (__all_sync(__activemask(), o2 + P <= g.K2)) {
+      stencil_sum<P, false>(grid, g, o0, iy, o2, iz, wx, dwx, wy, dwy, wz, dwz, pot, gx, gy, gz);
+    } else {
+      wrap_run<P>(o2, g.K2, iz);
+      stencil_sum<P, true>(grid, g, o0, iy, 0, iz, wx, dwx, wy, dwy, wz, dwz, pot, gx, gy, gz);
     }
     if (GRAD) {
       const double f = -w[a] * cc.iV;

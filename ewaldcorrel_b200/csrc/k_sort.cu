@@ -2,16 +2,18 @@
 //
 // The reference inserts every atom into a std::multimap keyed by
 // cid = (n0*K1 + n1)*K2 + n2; equal keys keep insertion order, so the result
-// is the STABLE sort of atoms by cid.  Here:
-//   1. key_hist_kernel: FP64 cell keys (rounding identical to the host, so
-//      boundary atoms land in the same cell), in-cell fractions, and the
-//      per-tile histogram of the first 8-bit digit;
-//   2. per digit: hist_scan_kernel (exclusive scan of that digit's tile
-//      histograms), then radix_scatter_kernel, which ranks ties in input
-//      order (stable by construction, so bit-exact against the CPU sort) and
-//      counts the NEXT digit of every key at the tile it lands in; the last
-//      pass also gathers the atom records into cell order;
-//   3. cell_start_kernel: first sorted rank of every cell.
+// is the STABLE sort of atoms by cid.  Two sorts produce that order here:
+//   - the main path (launch_cell_sort, below) is a counting sort over the
+//     cells, which also yields the per-cell offsets the spread needs;
+//   - the allocation-free entry point (end of file) is an LSD radix sort
+//     whose scratch is bounded by the atom count:
+//       1. key_hist_kernel: FP64 cell keys (rounding identical to the host,
+//          so boundary atoms land in the same cell), in-cell fractions, and
+//          the per-tile histogram of the first 8-bit digit;
+//       2. per digit: hist_scan_kernel (exclusive scan of that digit's tile
+//          histograms), then radix_scatter_kernel, which ranks ties in input
+//          order (stable by construction, so bit-exact against the CPU sort)
+//          and counts the NEXT digit of every key at the tile it lands in.
 // Integer counts only (their sums do not depend on order).
 #include <cstdio>
 #include <mutex>
@@ -187,35 +189,6 @@ __global__ void __launch_bounds__(RS_THREADS) radix_scatter_kernel(
   }
 }
 
-// cell_start[c] = first sorted rank whose key >= c, for c in [0, ncell].
-// With k(i) the sorted keys, k(-1) = -1 and k(n) = ncell, rank i is the
-// answer for exactly the cells (k(i-1), k(i)].  One warp takes 32 ranks:
-// it walks the contiguous cell range (k(i0-1), k(i0+31)] in chunks of 32
-// cells, each lane finding its cell's rank among the warp's 32 keys by a
-// register binary search (shuffles), so every store is coalesced and no
-// global search is needed.  Work: (n + ncell) / 32 warp steps.
-__global__ void __launch_bounds__(256) cell_start_kernel(int n, const uint32_t *__restrict__ keys, long ncell,
-                                                         int *__restrict__ cell_start) {
-  const long i0 = (((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-  const int lane = threadIdx.x & 31;
-  if (i0 > n) return;  // warp-uniform
-  const long i = i0 + lane;
-  const long kl = (i < n) ? (long)keys[i] : ncell;  // ranks beyond n: empty ranges at ncell
-  const long prev = (i0 == 0) ? -1 : (long)keys[i0 - 1];
-  const long last = __shfl_sync(0xffffffffu, kl, 31);
-  for (long cb = prev + 1; cb <= last; cb += 32) {
-    const long c = cb + lane;
-    // smallest l with k(i0 + l) >= c (exists for c <= last)
-    int l = 0;
-#pragma unroll
-    for (int step = 16; step >= 1; step >>= 1) {
-      const long kv = __shfl_sync(0xffffffffu, kl, l + step - 1);
-      if (kv < c) l += step;
-    }
-    if (c <= last) cell_start[c] = (int)(i0 + l);
-  }
-}
-
 static int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
 static int key_passes(long ncell) {
@@ -224,44 +197,284 @@ static int key_passes(long ncell) {
   return (bits + 7) / 8;
 }
 
-size_t sort_scratch_words(int cap, long ncell) {
-  const int ntiles = ceil_div(cap > 0 ? cap : 1, RS_TILE);
-  return (size_t)ntiles * RS_BINS * key_passes(ncell) + RS_MAX_PASSES * RS_BINS;
+// ---------------------------------------------------------------------------
+// Main-path cell sort: a counting sort over the cells.
+//
+//   1. key_count_kernel: keys and records (as above); every atom takes an
+//      arrival slot in its cell with an integer atomic (count[key]++).
+//   2. tile_sum_kernel + cell_offsets_kernel: exclusive scan of the per-cell
+//      counts, in place, into cell_start (cell_start[ncell] = n): the sum of
+//      every tile of 2^tshift cells, then each tile scans its cells from the
+//      sum of the tiles before it (at most ~2048 tiles, so that sum is short).
+//   3. cell_scatter_kernel: every atom goes to cell_start[key] + its arrival
+//      slot.  A cell holding one atom is final; the atoms of a shared cell
+//      sit in arrival order, which is not deterministic.
+//   4. cell_fixup_kernel: the atoms of each shared cell are put in input
+//      order (rank = number of the cell's atoms with a smaller index), which
+//      is exactly the stable order of the reference's multimap.  Cells with
+//      more than kBigCell atoms are listed and merge-sorted by the last CTA
+//      to finish (no waiting on other CTAs).
+// Only integer atomics (counts) are used; the result is the same bits on
+// every run.
+
+constexpr int kBigCell = 256;
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 16;
+constexpr int kScanChunk = kScanThreads * kScanItems;  // cells per CTA pass
+
+static int cell_tile_shift(long ncell) {
+  int s = 13;  // log2(kScanChunk)
+  while (((ncell + 1 + (1L << s) - 1) >> s) > 2048) s++;
+  return s;
+}
+static long cell_tiles(long ncell) {
+  const int s = cell_tile_shift(ncell);
+  return (ncell + 1 + (1L << s) - 1) >> s;
+}
+
+// Word layout of the cell-count region (the counts and the two control
+// words are zeroed before every sort):
+//   [0, ncell + 1)           counts, then offsets
+//   [ncell + 1, ncell + 3)   control: large cells, finished fix-up CTAs
+//   [ncell + 3, + T)         tile sums
+size_t cell_count_words(long ncell) { return (size_t)(ncell + 3 + cell_tiles(ncell)); }
+
+__global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const double *__restrict__ x,
+                                                        const double *__restrict__ w, uint32_t *__restrict__ keys,
+                                                        uint32_t *__restrict__ slot, float4 *__restrict__ rec,
+                                                        uint32_t *__restrict__ count) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const CellConst cc = *g.cell;
+  float4 r;
+  const uint32_t key = cell_key(g, cc, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
+  keys[a] = key;
+  rec[a] = r;
+  slot[a] = atomicAdd(&count[key], 1u);
+}
+
+// Block-wide sum (every thread gets the result); red: one word per warp.
+template <int NT>
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, uint32_t *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  uint32_t t = 0;
+#pragma unroll
+  for (int k = 0; k < NT / 32; k++) t += red[k];
+  return t;
+}
+
+// Loads kScanItems consecutive counts at c (16-byte aligned), zero past nscan.
+__device__ __forceinline__ bool load_counts(const uint32_t *cs, long c, long nscan, uint32_t (&a)[kScanItems]) {
+  const bool full = c + kScanItems - 1 < nscan;
+  if (full) {
+#pragma unroll
+    for (int v = 0; v < kScanItems / 4; v++) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(cs + c + 4 * v);
+      a[4 * v] = q.x; a[4 * v + 1] = q.y; a[4 * v + 2] = q.z; a[4 * v + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) a[k] = (c + k < nscan) ? cs[c + k] : 0u;
+  }
+  return full;
+}
+
+// tsum[t] = sum of the counts of tile t (cells [t << tshift, (t + 1) << tshift)).
+__global__ void __launch_bounds__(kScanThreads) tile_sum_kernel(const uint32_t *__restrict__ cs, long nscan,
+                                                                int tshift, uint32_t *__restrict__ tsum) {
+  __shared__ uint32_t red[kScanThreads / 32];
+  const long t0 = (long)blockIdx.x << tshift;
+  const long t1 = min(t0 + (1L << tshift), nscan);
+  uint32_t s = 0;
+  for (long c = t0 + (long)kScanItems * threadIdx.x; c < t1; c += kScanChunk) {
+    uint32_t a[kScanItems];
+    load_counts(cs, c, t1, a);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) s += a[k];
+  }
+  s = block_sum_u32<kScanThreads>(s, red);
+  if (threadIdx.x == 0) tsum[blockIdx.x] = s;
+}
+
+// cs[0 .. nscan): per-cell counts in, exclusive prefix sums out, one CTA per
+// tile; the tile's base is the sum of the earlier tiles' sums.
+__global__ void __launch_bounds__(kScanThreads) cell_offsets_kernel(uint32_t *__restrict__ cs, long nscan,
+                                                                    int tshift, const uint32_t *__restrict__ tsum) {
+  constexpr int NW = kScanThreads / 32;
+  __shared__ uint32_t wsum[NW];
+  __shared__ uint32_t red[NW];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t b = 0;
+  for (int i = threadIdx.x; i < (int)blockIdx.x; i += kScanThreads) b += tsum[i];
+  uint32_t run = block_sum_u32<kScanThreads>(b, red);
+  const long t0 = (long)blockIdx.x << tshift;
+  const long t1 = min(t0 + (1L << tshift), nscan);
+  for (long cb = t0; cb < t1; cb += kScanChunk) {
+    const long c = cb + (long)kScanItems * threadIdx.x;
+    uint32_t a[kScanItems];
+    const bool full = load_counts(cs, c, t1, a);
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) s += a[k];
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    __syncthreads();  // wsum of the previous pass has been read
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0, blk = 0;
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+      const uint32_t ws = wsum[k];
+      if (k < warp) wpre += ws;
+      blk += ws;
+    }
+    uint32_t e = run + wpre + incl - s;
+    uint32_t o[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+      o[k] = e;
+      e += a[k];
+    }
+    if (full) {
+#pragma unroll
+      for (int v = 0; v < kScanItems / 4; v++)
+        *reinterpret_cast<uint4 *>(cs + c + 4 * v) = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kScanItems; k++)
+        if (c + k < t1) cs[c + k] = o[k];
+    }
+    run += blk;
+  }
+}
+
+__global__ void __launch_bounds__(256) cell_scatter_kernel(int n, const uint32_t *__restrict__ keys,
+                                                           const uint32_t *__restrict__ slot,
+                                                           const float4 *__restrict__ rec,
+                                                           const int *__restrict__ cs, uint32_t *__restrict__ skeys,
+                                                           uint32_t *__restrict__ perm, uint32_t *__restrict__ tmp,
+                                                           float4 *__restrict__ rec_sorted) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const uint32_t key = keys[a];
+  const int lo = cs[key], hi = cs[key + 1];
+  const int pos = lo + (int)slot[a];
+  skeys[pos] = key;
+  if (hi - lo == 1) {
+    perm[pos] = (uint32_t)a;
+    rec_sorted[pos] = rec[a];
+  } else {
+    tmp[pos] = (uint32_t)a;
+  }
+}
+
+// Merge sort of one large cell's atom indices (distinct values) by one CTA,
+// ping-ponging between tmp[lo..) and perm[lo..); then the records.
+__device__ void big_cell_sort(int lo, int c, uint32_t *tmp, uint32_t *perm, const float4 *__restrict__ rec,
+                              float4 *__restrict__ rec_sorted) {
+  uint32_t *src = tmp + lo, *dst = perm + lo;
+  for (int wd = 1; wd < c; wd <<= 1) {
+    for (int i = threadIdx.x; i < c; i += blockDim.x) {
+      const int run = i / wd, rs = run * wd;
+      const bool left = (run & 1) == 0;
+      const int os = left ? rs + wd : rs - wd;  // partner run
+      const int oe = min(os + wd, c);
+      const uint32_t v = src[i];
+      int l = os, h = (os < c) ? oe : os;  // number of partner values below v
+      while (l < h) {
+        const int m = (l + h) >> 1;
+        if (src[m] < v) l = m + 1; else h = m;
+      }
+      dst[(left ? rs : os) + (i - rs) + (l - os)] = v;
+    }
+    __syncthreads();
+    uint32_t *t = src;
+    src = dst;
+    dst = t;
+  }
+  for (int i = threadIdx.x; i < c; i += blockDim.x) {
+    const uint32_t a = src[i];
+    perm[lo + i] = a;
+    rec_sorted[lo + i] = rec[a];
+  }
+  __syncthreads();
+}
+
+// ctl[0]: number of listed large cells, ctl[1]: finished CTAs (both zero on
+// entry; the last CTA resets ctl[1]).  big: listed cell keys (capacity n).
+__global__ void __launch_bounds__(256) cell_fixup_kernel(int n, const uint32_t *__restrict__ skeys,
+                                                         const int *__restrict__ cs, uint32_t *tmp, uint32_t *perm,
+                                                         const float4 *__restrict__ rec,
+                                                         float4 *__restrict__ rec_sorted, uint32_t *ctl,
+                                                         uint32_t *big) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const uint32_t key = skeys[i];
+    const int lo = cs[key], c = cs[key + 1] - lo;
+    if (c > kBigCell) {
+      if (i == lo) big[atomicAdd(&ctl[0], 1u)] = key;
+    } else if (c > 1) {
+      const uint32_t a = tmp[i];
+      int r = 0;
+      for (int j = lo; j < lo + c; j++) r += (tmp[j] < a) ? 1 : 0;
+      perm[lo + r] = a;
+      rec_sorted[lo + r] = rec[a];
+    }
+  }
+  // the last CTA to finish sorts the listed large cells
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&ctl[1], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const uint32_t nb = *((volatile uint32_t *)&ctl[0]);
+  for (uint32_t b = 0; b < nb; b++) {
+    const uint32_t key = *((volatile uint32_t *)&big[b]);
+    const int lo = cs[key], c = cs[key + 1] - lo;
+    big_cell_sort(lo, c, tmp, perm, rec, rec_sorted);
+  }
+  if (threadIdx.x == 0) ctl[1] = 0u;
 }
 
 // Computes keys/fractions, sorts, and builds the per-cell offsets.
-// On return (stream order): keys[cur] / vals[cur] hold the stable order,
+// On return (stream order): keys[0] / vals[0] hold the stable order,
 // rec_sorted the records in that order, cell_start the cell offsets.
 int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
                      cudaStream_t st) {
   const long ncell = (long)g.K0 * g.K1 * g.K2;
-  int launches = 0;
+  const long ntiles = cell_tiles(ncell);
+  const int tshift = cell_tile_shift(ncell);
+  uint32_t *count = reinterpret_cast<uint32_t *>(b.cell_start);
+  uint32_t *ctl = count + (ncell + 1);
+  uint32_t *tsum = count + (ncell + 3);
   b.cur = 0;
+  cudaMemsetAsync(count, 0, sizeof(uint32_t) * (ncell + 3), st);
+  int launches = 0;
   if (n > 0) {
-    const int npass = key_passes(ncell);
-    const int ntiles = ceil_div(n, RS_TILE);
-    uint32_t *totals = b.hist + (size_t)ntiles * RS_BINS * npass;
-    cudaMemsetAsync(totals, 0, sizeof(uint32_t) * RS_BINS * npass, st);
-    key_hist_kernel<<<ntiles, RS_THREADS, 0, st>>>(g, n, x, w, b.keys[1], b.rec, b.hist, ntiles, npass, totals);
+    key_count_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[1], b.vals[1], b.rec, count);
     launches++;
-    // keys live in keys[1] before the first pass; passes alternate 1 -> 0 -> 1 ...
-    int src = 1;
-    for (int p = 0; p < npass; p++) {
-      const int dst = src ^ 1;
-      const bool last = (p == npass - 1);
-      uint32_t *hp = b.hist + (size_t)p * RS_BINS * ntiles;
-      hist_scan_kernel<<<RS_BINS, 256, 0, st>>>(hp, ntiles, totals + p * RS_BINS);
-      radix_scatter_kernel<<<ntiles, RS_THREADS, 0, st>>>(
-          b.keys[src], p == 0 ? nullptr : b.vals[src], b.keys[dst], b.vals[dst], n, 8 * p, hp, ntiles,
-          last ? nullptr : hp + (size_t)RS_BINS * ntiles, b.rec, last ? b.rec_sorted : nullptr);
-      launches += 2;
-      src = dst;
-    }
-    b.cur = src;
   }
-  cell_start_kernel<<<ceil_div(ceil_div((long)n + 1, 32) * 32, 256), 256, 0, st>>>(n, b.keys[b.cur], ncell,
-                                                                                      b.cell_start);
-  return launches + 1;
+  tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, ncell + 1, tshift, tsum);
+  cell_offsets_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, ncell + 1, tshift, tsum);
+  launches += 2;
+  if (n > 0) {
+    cell_scatter_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[1], b.vals[1], b.rec, b.cell_start, b.keys[0],
+                                                          b.vals[0], b.tmp, b.rec_sorted);
+    cell_fixup_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[0], b.cell_start, b.tmp, b.vals[0], b.rec,
+                                                        b.rec_sorted, ctl, b.hist);
+    launches += 2;
+  }
+  return launches;
 }
 
 }  // namespace spme

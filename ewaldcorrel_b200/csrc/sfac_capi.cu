@@ -153,6 +153,7 @@ void free_atoms(Handle *h) {
     dfree(h->sb.keys[i]);
     dfree(h->sb.vals[i]);
   }
+  dfree(h->sb.tmp);
   dfree(h->sb.rec);
   dfree(h->sb.rec_sorted);
   dfree(h->sb.hist);
@@ -165,8 +166,8 @@ bool ensure_atoms(Handle *h, int n) {
   const int cap = n + n / 2 + 64;
   bool ok = dalloc(h, &h->d_x, 3 * (size_t)cap) && dalloc(h, &h->d_w, cap);
   for (int i = 0; i < 2; i++) ok = ok && dalloc(h, &h->sb.keys[i], cap) && dalloc(h, &h->sb.vals[i], cap);
-  ok = ok && dalloc(h, &h->sb.rec, cap) && dalloc(h, &h->sb.rec_sorted, cap) &&
-       dalloc(h, &h->sb.hist, sort_scratch_words(cap, h->ncell));
+  ok = ok && dalloc(h, &h->sb.tmp, cap) && dalloc(h, &h->sb.rec, cap) && dalloc(h, &h->sb.rec_sorted, cap) &&
+       dalloc(h, &h->sb.hist, cap);
   if (!ok) {
     free_atoms(h);
     return false;
@@ -296,7 +297,7 @@ void *sfac_ctor(double L[6], int K[3], int order) {
                   kRedWords) &&
        dalloc(h, &h->d_red, kRedWords) && dalloc(h, &h->d_ev, kRedWords) && dalloc(h, &h->d_cell, 1) &&
        dalloc(h, &h->d_ic, 1) &&
-       dalloc(h, &h->sb.cell_start, ncell + 1);
+       dalloc(h, &h->sb.cell_start, cell_count_words(ncell));
   for (int d = 0; d < 3 && ok; d++) ok = dalloc(h, &h->d_iB[d], K[d]) && dalloc(h, &h->d_tw[d], K[d]);
   const size_t hf = (size_t)(2 * h->nmodes > h->nreal ? 2 * h->nmodes : h->nreal);
   ok = ok && CK(h, cudaMallocHost((void **)&h->h_S, sizeof(double) * 2 * h->nmodes)) &&
@@ -539,7 +540,8 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   const bool fresh = !h->d_rows;
   if (!h->d_rows && !dalloc(h, &h->d_rows, (size_t)h->K[0] * h->K[1])) return 2;
   const CellConst &c = h->hcell;
-  h->hic = InfConst{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, beta, max_m};
+  const double pb = 3.14159265358979323846 / beta;
+  h->hic = InfConst{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, beta, max_m, -(pb * pb)};
   Influence &inf = h->inf;
   inf = Influence{};
   inf.mode = 2;
@@ -696,10 +698,10 @@ int sfac_set_tuning(void *p, int key, int value) {
 unsigned long sfac_footprint_bytes(const int K[3], int n) {
   const size_t K0 = K[0], K1 = K[1], K2 = K[2], ldim = K2 / 2 + 1, nn = (size_t)(n > 0 ? n : 1);
   const size_t cap = nn + nn / 2 + 64;
-  size_t b = 4 * K0 * K1 * K2 + 8 * K0 * K1 * ldim + 4 * (K0 * K1 * K2 + 1);  // grids + cell offsets
+  size_t b = 4 * K0 * K1 * K2 + 8 * K0 * K1 * ldim + 4 * cell_count_words((long)(K0 * K1 * K2));  // grids, cells
   b += (K0 + K1 + K2) * 16 + sizeof(RowImg) * K0 * K1;                   // moduli, twiddles, rows
   b += 8 * (size_t)fft_x_blocks_max(K[1], K[2]) * kRedWords;               // partials
-  b += cap * (24 + 8 + 16 + 16 + 16);                                      // sort buffers, records
+  b += cap * (24 + 8 + 6 * 4 + 16 + 16);                                   // sort buffers, records
   b += 8 * cap * 8;                                                        // gather staging
   b += 8 * 2 * K0 * K1 * ldim + 4 * K0 * K1 * K2;                          // host mirrors (pinned)
   return b;

@@ -11,15 +11,16 @@ namespace spme {
 
 // ---- sort (k_sort.cu) ----
 struct SortBuffers {
-  uint32_t *keys[2];   // ping-pong key buffers (cap)
-  uint32_t *vals[2];   // ping-pong original indices (cap)
+  uint32_t *keys[2];   // [1]: cell key of every atom (input order); [0]: keys in cell order
+  uint32_t *vals[2];   // [1]: arrival slot of every atom in its cell; [0]: the stable permutation
+  uint32_t *tmp;       // cell-order slots of shared cells, in arrival order (cap)
   float4 *rec;         // (frac0, frac1, frac2, charge) in input order (cap)
   float4 *rec_sorted;  // the same in cell order (cap)
-  uint32_t *hist;      // radix histograms (sort_scratch_words(cap))
-  int *cell_start;     // K0*K1*K2 + 1 offsets into the sorted order
-  int cur;             // which keys/vals buffer holds the sorted result
+  uint32_t *hist;      // keys of cells too large for the in-place fix-up (cap)
+  int *cell_start;     // cell_count_words(ncell): K0*K1*K2 + 1 counts -> offsets, tile counts, control words
+  int cur;             // which keys/vals buffer holds the sorted result (0)
 };
-size_t sort_scratch_words(int cap, long ncell);
+size_t cell_count_words(long ncell);
 int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
                       cudaStream_t st);
 
@@ -93,9 +94,10 @@ struct RowImg {
 
 // Constants of the device Ewald influence function (device memory): the
 // cell used for m = iL n (the one current when the function was set; later
-// box changes do not touch it, as with set_A) and the Ewald parameters.
+// box changes do not touch it, as with set_A), the Ewald parameters and the
+// exponent factor fac = -(pi / beta)^2.
 struct InfConst {
-  double iL00, iL10, iL11, iL20, iL21, iL22, beta, max_m;
+  double iL00, iL10, iL11, iL20, iL21, iL22, beta, max_m, fac;
 };
 
 // Influence function source for the convolution.

@@ -158,10 +158,17 @@ def _sort_inputs():
     out.append(("plain1000", c1.L, c1.K, c1.x))
     c2 = configs.cfg2_water()
     out.append(("water98304", c2.L, c2.K, c2.x))
+    # cells with more atoms than the in-place fix-up takes (two large cells,
+    # 2000 and 300 atoms, among scattered ones), and one cell holding every
+    # atom at the same point
+    big = np.concatenate([rng.uniform(0, 2, size=(700, 3)), 0.51 + rng.uniform(0, 0.1, size=(2000, 3)),
+                          rng.uniform(0, 2, size=(300, 3)), 1.26 + rng.uniform(0, 0.1, size=(300, 3))])
+    out.append(("large_cells", Lc, K, rng.permutation(big)))
+    out.append(("one_cell", Lc, K, np.full((4097, 3), 0.7)))
     return out
 
 
-@pytest.mark.parametrize("case", range(5))
+@pytest.mark.parametrize("case", range(7))
 def test_cell_sort_bit_exact(case):
     name, L, K, x = _sort_inputs()[case]
     ew = E()
