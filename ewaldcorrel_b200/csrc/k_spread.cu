@@ -58,25 +58,39 @@ template <int P>
 struct SpreadSmem {
   static constexpr int H = P / 2;
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
-  static constexpr int WS = 3 * P + 1;  // staged row stride (odd: no bank conflicts)
+  // Staged atom, read by every lane in the walk:
+  //   zq: (rel bits, wz[0..P-1], pad) as float4s -- broadcast loads;
+  //   wx: q*M(fx+i) at [3 + i], zero elsewhere, so lane cx reads [rx - cx + 3]
+  //       with no range test (rx - cx in [-3, RX - 1]);
+  //   wy: M(fy+j) at [7 + j], zero elsewhere, read at [ry - cy + 7].
+  // The zero entries are written once per CTA; staging writes only the P
+  // weights of each axis.  Odd row strides keep the lane-per-atom staging
+  // stores free of bank conflicts.
+  static constexpr int NZ4 = (P + 1 + 3) / 4;
+  static constexpr int WXS = (P + 6) | 1, WYS = (P + 14) | 1;
   int start[NR];                         // first sorted atom of each halo row segment
   int pref[NR + 1];                      // prefix sums of the row segment counts
-  int rel[SP_WARPS][32];                 // staged atom: rx | ry << 8 | (rz + 64) << 16
-  float wt[SP_WARPS][32][WS];            // staged atom: q*M(fx+i), M(fy+j), M(fz+P-1-t)
-  float part[SP_WARPS][SP_TZ][33];       // per-warp partial bricks for the final sum
+  union {
+    struct {
+      float4 zq[SP_WARPS][32][NZ4];
+      float wx[SP_WARPS][32][WXS];
+      float wy[SP_WARPS][32][WYS];
+    } st;                                // staging (walk phase)
+    float part[SP_WARPS][SP_TZ][33];     // per-warp partial bricks for the final sum
+  };
 };
 
 // One CTA per 4 x 8 x 32 brick; its 4 warps take the brick's staged atoms in
 // round-robin chunks of 32 and keep private register accumulators, summed in
 // warp order at the end (fixed order: deterministic).
 template <int P>
-__global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Spline S, const int *__restrict__ cs,
+__global__ void __launch_bounds__(SP_WARPS * 32, 8) spread_reg_kernel(Geom g, Spline S, const int *__restrict__ cs,
                                                                   const uint32_t *__restrict__ keys,
                                                                   const float4 *__restrict__ rec,
                                                                   float *__restrict__ grid, int ntx, int nty,
-                                                                  int ntz) {
+                                                                  int ntz, FastDiv K2d) {
   using SM = SpreadSmem<P>;
-  constexpr int H = SM::H, RY = SM::RY, NR = SM::NR;
+  constexpr int H = SM::H, RY = SM::RY, NR = SM::NR, NZ4 = SM::NZ4;
   __shared__ SM s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long tile = blockIdx.x;
@@ -84,6 +98,11 @@ __global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Splin
   const int x0 = tx * SP_TX, y0 = ty * SP_TY, z0 = tz * SP_TZ;
   const int cx = lane >> 3, cy = lane & 7;
   const int K0 = g.K0, K1 = g.K1, K2 = g.K2;
+
+  // zero the padded weight rows once (the staged weights overwrite only the
+  // fixed non-zero positions)
+  for (int i = threadIdx.x; i < SP_WARPS * 32 * SM::WXS; i += SP_WARPS * 32) (&s.st.wx[0][0][0])[i] = 0.f;
+  for (int i = threadIdx.x; i < SP_WARPS * 32 * SM::WYS; i += SP_WARPS * 32) (&s.st.wy[0][0][0])[i] = 0.f;
 
   float acc[SP_TZ];
 #pragma unroll
@@ -121,6 +140,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Splin
     }
     __syncthreads();
     const int total = s.pref[NR];
+    const int zoff = ezs + H - (P - 1) - z0 - n2a;  // rz = n2 + zoff
     for (int chunk = warp * 32; chunk < total; chunk += SP_WARPS * 32) {
       const int t = chunk + lane;
       if (t < total) {
@@ -131,30 +151,40 @@ __global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Splin
         }
         const int a = s.start[lo] + (t - s.pref[lo]);
         const float4 u = __ldg(rec + a);
-        const int n2 = (int)(__ldg(keys + a) % (uint32_t)K2);
+        uint32_t qk, n2;
+        K2d.divmod(__ldg(keys + a), qk, n2);
         const int rx = lo / RY, ry = lo % RY;
-        const int rz = ezs + (n2 - n2a) + H - (P - 1) - z0;
-        s.rel[warp][lane] = rx | (ry << 8) | ((rz + 64) << 16);
-        float *wt = s.wt[warp][lane];
+        const int rz = (int)n2 + zoff;
+        float zw[4 * NZ4];
+        zw[0] = __int_as_float(rx | (ry << 8) | ((rz + 64) << 16));
 #pragma unroll
         for (int i = 0; i < P; i++) {
-          wt[i] = u.w * bspl_eval(S, P, u.x, i);
-          wt[P + i] = bspl_eval(S, P, u.y, i);
-          wt[2 * P + i] = bspl_eval(S, P, u.z, P - 1 - i);
+          s.st.wx[warp][lane][3 + i] = u.w * bspl_eval(S, P, u.x, i);
+          s.st.wy[warp][lane][7 + i] = bspl_eval(S, P, u.y, i);
+          zw[1 + i] = bspl_eval(S, P, u.z, P - 1 - i);
         }
+#pragma unroll
+        for (int i = P + 1; i < 4 * NZ4; i++) zw[i] = 0.f;
+#pragma unroll
+        for (int v = 0; v < NZ4; v++) s.st.zq[warp][lane][v] = make_float4(zw[4 * v], zw[4 * v + 1], zw[4 * v + 2], zw[4 * v + 3]);
       }
       __syncwarp();
       const int na = min(32, total - chunk);
+      const float *wxl = &s.st.wx[warp][0][3 - cx];
+      const float *wyl = &s.st.wy[warp][0][7 - cy];
       for (int a = 0; a < na; a++) {
-        const int rel = s.rel[warp][a];
-        const float *wt = s.wt[warp][a];
-        const int i = (rel & 0xff) - cx, j = ((rel >> 8) & 0xff) - cy;
-        const int rz = (rel >> 16) - 64;
-        const bool ok = (unsigned)i < (unsigned)P && (unsigned)j < (unsigned)P;
-        const float w = ok ? wt[ok ? i : 0] * wt[P + (ok ? j : 0)] : 0.f;
+        float zw[4 * NZ4];
+#pragma unroll
+        for (int v = 0; v < NZ4; v++) {
+          const float4 q = s.st.zq[warp][a][v];
+          zw[4 * v] = q.x; zw[4 * v + 1] = q.y; zw[4 * v + 2] = q.z; zw[4 * v + 3] = q.w;
+        }
+        const int rel = __float_as_int(zw[0]);
+        const int rx = rel & 0xff, ry = (rel >> 8) & 0xff, rz = (rel >> 16) - 64;
+        const float w = wxl[a * SM::WXS + rx] * wyl[a * SM::WYS + ry];
         float wz[P];
 #pragma unroll
-        for (int q = 0; q < P; q++) wz[q] = wt[2 * P + q];
+        for (int q = 0; q < P; q++) wz[q] = zw[1 + q];
         z_dispatch<P>(rz, acc, w, wz);
       }
       __syncwarp();
@@ -162,7 +192,9 @@ __global__ void __launch_bounds__(SP_WARPS * 32) spread_reg_kernel(Geom g, Splin
     ezs += len;
   }
 
-  // partial bricks to shared memory, then the fixed-order sum over warps
+  // partial bricks to shared memory (over the staging arrays), then the
+  // fixed-order sum over warps
+  __syncthreads();
 #pragma unroll
   for (int z = 0; z < SP_TZ; z++) s.part[warp][z][lane] = acc[z];
   __syncthreads();
@@ -181,7 +213,8 @@ static void spread_p(const Geom &g, const Spline &S, const int *cs, const uint32
                      float *grid, cudaStream_t st) {
   const int ntx = (g.K0 + SP_TX - 1) / SP_TX, nty = (g.K1 + SP_TY - 1) / SP_TY, ntz = (g.K2 + SP_TZ - 1) / SP_TZ;
   const long tiles = (long)ntx * nty * ntz;
-  spread_reg_kernel<P><<<(unsigned)tiles, SP_WARPS * 32, 0, st>>>(g, S, cs, keys, rec, grid, ntx, nty, ntz);
+  spread_reg_kernel<P><<<(unsigned)tiles, SP_WARPS * 32, 0, st>>>(g, S, cs, keys, rec, grid, ntx, nty, ntz,
+                                                                  FastDiv((uint32_t)g.K2));
 }
 
 int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
