@@ -53,33 +53,68 @@ def _env_int(name, default):
 
 # ------------------------------------------------------------ clocks --
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+    """SM clocks and throttle reasons sampled while the GPU works: an NVML
+    polling thread (every 2 ms, so that a timed region of a few milliseconds
+    still gets samples), with `nvidia-smi -lms 100` written beside it to
+    gpurun_out/clocks_rank<i>.csv as a second record."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.samples = []  # (sm_mhz, reasons bitmask)
+        self.smax = None
+        self._stop = None
+        self._thread = None
+
+    def _poll(self):
+        import pynvml
+
+        try:
+            pynvml.nvmlInit()
+            hnd = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(hnd, pynvml.NVML_CLOCK_SM))
+            while not self._stop.is_set():
+                sm = pynvml.nvmlDeviceGetClockInfo(hnd, pynvml.NVML_CLOCK_SM)
+                rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(hnd)
+                self.samples.append((float(sm), int(rs)))
+                self._stop.wait(0.002)
+        except Exception:
+            pass
 
     def __enter__(self):
+        import threading
+
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._poll, daemon=True)
+        self._thread.start()
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
-            # wait (bounded) for the first sample so the timed region is covered
-            t0 = time.time()
-            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
-                time.sleep(0.05)
         except Exception:
             self.proc = None
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and not self.samples:
+            time.sleep(0.01)
         return self
 
+    def mark(self):
+        """Index of the next sample (to summarise only part of the run)."""
+        return len(self.samples)
+
     def __exit__(self, *a):
+        if self._stop is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -88,27 +123,13 @@ class ClockSampler:
                 self.proc.kill()
             self.f.close()
 
-    def summary(self):
-        if self.proc is None or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            p = [t.strip() for t in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                smax = float(p[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+    def summary(self, start=0, end=None):
+        smp = self.samples[start:end]
+        if not smp:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["unsampled"], "samples": 0}
+        reasons = sorted(n for n, bit in self.REASONS.items() if any(r & bit for _, r in smp))
+        return {"sm_mhz": statistics.median(s for s, _ in smp), "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(smp), "source": "NVML, 2 ms polling during the timed steps"}
 
 
 # ------------------------------------------------- algorithmic bytes --
@@ -132,6 +153,30 @@ def algorithmic_bytes(n, K):
         "gather": G + atom_in + atom_out,
         "solve_total": 2 * atom_in + atom_out + 4 * G + 2 * H,
     }
+
+
+# DRAM bytes (read + write) per launch of each stage's kernels, from one ncu
+# capture of a plain solve (ncu --metrics dram__bytes_read.sum,
+# dram__bytes_write.sum,gpu__time_duration.sum; cold caches; summarised in
+# profiles/dram_per_kernel_water_triclinic.md).  Writes that stay in the
+# 126 MB L2 past the kernel's end are not counted by the capture.
+NCU_TRAFFIC = {
+    "water": {"cell_sort": 24.22e6, "spread": 5.53e6, "fft_forward": 7.30e6, "convolution": 5.25e6,
+              "fft_inverse": 7.41e6, "gather": 6.70e6},
+    "triclinic": {"cell_sort": 437.62e6, "spread": 124.25e6, "fft_forward": 163.73e6, "convolution": 91.46e6,
+                  "fft_inverse": 166.82e6, "gather": 158.28e6},
+}
+# Kernels of each stage (the roofline is reported for the longest stage that
+# is a single kernel launch).
+STAGE_KERNELS = {
+    "cell_sort": "key_count + tile_sum + cell_offsets + cell_scatter + cell_fixup (+ memset)",
+    "spread": "spread_reg_kernel",
+    "fft_forward": "fft_zr2c2_kernel + fft_y2_kernel<-1>",
+    "convolution": "fft_x2_kernel<XM_FWD_CONV_INV> (x FFT, Ewald convolution, energy/virial, inverse x FFT)",
+    "fft_inverse": "fft_y2_kernel<+1> (+ energy/virial reduction) + fft_zc2r2_kernel",
+    "gather": "gather_kernel (forces + potentials)",
+}
+SINGLE_KERNEL_STAGES = ("spread", "convolution", "gather")
 
 
 def measured_peak():
@@ -247,6 +292,7 @@ def run_b200(args, rank, world, local_rank):
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     l0 = solver.launches()
     barrier()
+    c0 = clk.mark()
     with torch.cuda.stream(stream):
         for k in range(K):
             flush.zero_()
@@ -254,6 +300,7 @@ def run_b200(args, rank, world, local_rank):
             solver.solve(x, q, dx, phi, ev)
             ends[k].record(stream)
     barrier()
+    c1 = clk.mark()
     launches = solver.launches() - l0
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(step_ms)
@@ -277,7 +324,7 @@ def run_b200(args, rank, world, local_rank):
             stage_acc[s_].append(v)
     stage_ms = {s_: statistics.mean(v) for s_, v in stage_acc.items()}
     alg = algorithmic_bytes(n, c.K)
-    dominant = max(STAGES, key=lambda s_: stage_ms[s_])
+    dominant = max(SINGLE_KERNEL_STAGES, key=lambda s_: stage_ms[s_])
     peak, peak_kind = measured_peak()
     achieved = alg[dominant] / (stage_ms[dominant] / 1e3) / 1e9
 
@@ -306,6 +353,8 @@ def run_b200(args, rank, world, local_rank):
         e2e_ms.append((time.perf_counter() - a) * 1e3)
     clk.__exit__(None, None, None)
     clocks = clk.summary()
+    clocks["window"] = "warm-up, timed steps, per-stage timing and the e2e run"
+    clocks["timed_steps"] = clk.summary(c0, c1)
     e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
@@ -336,14 +385,16 @@ def run_b200(args, rank, world, local_rank):
         },
         "latency_ms": {"p50": p50, "p99": p99, "mean": total_ms_max / K},
         "stage_ms": stage_ms,
+        "stage_kernels": STAGE_KERNELS,
         "roofline": {
             "bound": "hbm",
-            "kernel": dominant,
+            "kernel": f"{dominant}: {STAGE_KERNELS[dominant]}",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
-            "traffic": None,
+            "traffic": NCU_TRAFFIC.get(args.workload, {}).get(dominant),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch (profiles/)",
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
             "algorithmic_bytes": alg[dominant],
             "solve_algorithmic_bytes": alg["solve_total"],

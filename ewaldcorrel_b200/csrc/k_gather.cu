@@ -81,7 +81,7 @@ struct SortedView {
 // origin shifted by one cell, whose extra weight M(0) = 0 -- the same sum);
 // otherwise the origin comes from x in FP64 exactly as de2/potl compute it.
 template <int P, bool GRAD, bool POT, bool CELL, bool SORTED>
-__global__ void __launch_bounds__(256) gather_kernel(Geom g, Spline S, int n, const double *__restrict__ x,
+__global__ void __launch_bounds__(256, CELL ? 2 : 3) gather_kernel(Geom g, Spline S, int n, const double *__restrict__ x,
                                                      const double *__restrict__ w,
                                                      const float *__restrict__ grid, double *__restrict__ dx,
                                                      double *__restrict__ phi, double *__restrict__ cellp,
