@@ -95,6 +95,32 @@ int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStr
   return 1;
 }
 
+// Tabulates the device Ewald influence function (inf.mode 2) per stored
+// mode in the layout of set_A's tables: A[i] and dA[6 i + c] (FP64), so the
+// solves read them instead of evaluating the images of every mode again.
+__global__ void __launch_bounds__(256) ewald_table_kernel(Geom g, Influence inf, double *__restrict__ A,
+                                                          double *__restrict__ dA) {
+  const long nmodes = (long)g.K0 * g.K1 * g.ldim;
+  const InfConst ic = *inf.ic;
+  const bool even = (g.K2 % 2) == 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nmodes; i += (long)gridDim.x * blockDim.x) {
+    const int kz = (int)(i % g.ldim);
+    const long r = i / g.ldim;
+    const int ky = (int)(r % g.K1), kx = (int)(r / g.K1);
+    const bool plane = (kz == 0) || (even && kz == g.ldim - 1);
+    double a, d[6];
+    mode_influence(inf, ic, g, i, kx, ky, kz, plane, a, d);
+    A[i] = a;
+#pragma unroll
+    for (int c = 0; c < 6; c++) dA[6 * i + c] = d[c];
+  }
+}
+
+int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *dA, cudaStream_t st) {
+  ewald_table_kernel<<<4 * 148, 256, 0, st>>>(g, inf, A, dA);
+  return 1;
+}
+
 int launch_finish(const double *partials, int nblocks, const CellConst *cell, double *raw, double *ev,
                   cudaStream_t st) {
   conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, nblocks, cell, raw, ev);

@@ -426,6 +426,41 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
             data[line + (long)kx * nlines] = cscale(w[k2], (float)(iB0[kx] * s12));
           }
         }
+      } else if (inf.mode == 1) {
+        // tabulated influence function: the line's values stay in registers
+        // and all R modes' table loads are in flight together
+        if (live) {
+          const bool even = (g.K2 % 2) == 0;
+          const bool plane = (kz == 0) || (even && kz == ldim - 1);
+          const double s12 = iB1[ky] * iB2[kz];
+#pragma unroll
+          for (int k2 = 0; k2 < R; k2++) {
+            const int kx = k1 + n1 * k2;
+            const long i = ((long)kx * K1 + ky) * ldim + kz;
+            const float2 q = w[k2];
+            const double ib = iB0[kx] * s12;
+            double sq = (double)q.x * q.x + (double)q.y * q.y;
+            if (MODE == XM_FWD_CONV_INV) sq *= ib * ib;  // |F iB|^2
+            const double A = inf.A[i];
+            acc[0] += sq * A;
+#pragma unroll
+            for (int c = 0; c < 6; c++) acc[1 + c] += sq * inf.dA[6 * i + c];
+            if (MODE != XM_EN) {
+              double f = A * ib * (MODE == XM_FWD_CONV_INV ? ib : 1.0);
+              if (plane) f *= 2.0;
+              w[k2] = cscale(q, (float)f);
+            }
+          }
+        }
+        if (MODE != XM_EN) {
+          rdft::dft<R, +1>(w);
+#pragma unroll
+          for (int j2 = 0; j2 < R; j2++) {
+            float2 c = tw[j2 * k1];
+            c.y = -c.y;
+            ex[(k1 * n2 + j2) * B + b] = cmul(w[j2], c);
+          }
+        }
       } else {
         // the pointwise step walks the line's values through the thread's
         // own exchange slots (a run-time index into registers would spill)

@@ -78,6 +78,11 @@ struct Handle {
 
 Handle *H(void *p) { return reinterpret_cast<Handle *>(p); }
 
+// Largest tabulated device Ewald influence function (A + 6 dA, FP64): a
+// table that stays in L2 is cheaper to read than the images are to evaluate;
+// a larger one streamed from HBM every solve is not.
+constexpr size_t kEwaldTableMaxBytes = (size_t)64 << 20;  // stays resident in the 126 MB L2
+
 bool check(Handle *h, cudaError_t e, const char *what) {
   if (e == cudaSuccess) return true;
   if (h) {
@@ -537,13 +542,11 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
     printf("sfac_set_ewald: bad beta %g or max_m %g\n", beta, max_m);
     return 1;
   }
-  const bool fresh = !h->d_rows;
   if (!h->d_rows && !dalloc(h, &h->d_rows, (size_t)h->K[0] * h->K[1])) return 2;
   const CellConst &c = h->hcell;
   const double pb = 3.14159265358979323846 / beta;
   h->hic = InfConst{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, beta, max_m, -(pb * pb)};
-  Influence &inf = h->inf;
-  inf = Influence{};
+  Influence inf{};
   inf.mode = 2;
   inf.ic = h->d_ic;
   inf.rows = h->d_rows;
@@ -551,9 +554,26 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   // constants and row tables are rewritten in place on the stream: later
   // solves see them without new kernel arguments
   if (!CK(h, cudaMemcpyAsync(h->d_ic, &h->hic, sizeof(InfConst), cudaMemcpyHostToDevice, h->stream))) return 3;
-  const int k = launch_ewald_rows(h->geom, inf, h->d_rows, h->stream);
+  int k = launch_ewald_rows(h->geom, inf, h->d_rows, h->stream);
+  // Tabulate A and dA once (FP64, 56 bytes per stored mode) when the tables
+  // stay within kEwaldTableMaxBytes: every solve then reads them instead of
+  // evaluating the images (one exp each) of every mode.  SFAC_EWALD_TABLE=0
+  // keeps the per-solve evaluation.
+  const size_t nm = (size_t)h->nmodes;
+  bool table = 56 * nm <= kEwaldTableMaxBytes;
+  if (const char *e = getenv("SFAC_EWALD_TABLE")) table = table && !(e[0] == '0' && e[1] == 0);
+  if (table) {
+    if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
+    k += launch_ewald_table(h->geom, inf, h->d_A, h->d_A + nm, h->stream);
+    inf = Influence{};
+    inf.mode = 1;
+    inf.A = h->d_A;
+    inf.dA = h->d_A + nm;
+    inf.K2d = FastDiv((uint32_t)h->K[2]);
+  }
   if (!launched(h, k, "ewald rows")) return 3;
-  if (fresh || h->a_mode != 2) h->version++;
+  if (h->a_mode != 2 || memcmp(&inf, &h->inf, sizeof(Influence)) != 0) h->version++;  // kernel arguments changed
+  h->inf = inf;
   h->a_mode = 2;
   return 0;
 }

@@ -111,6 +111,9 @@ struct Influence {
 };
 // Builds the row image tables of an Ewald influence function (mode 2).
 int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStream_t st);
+// Tabulates a mode-2 influence function as FP64 tables A (nmodes) and dA
+// (6 per mode), the layout of mode 1.
+int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *dA, cudaStream_t st);
 constexpr int kConvBlocks = 592;  // 4 x 148 SMs: fixed, so the reduction order is fixed
 constexpr int kRedWords = 8;      // e, v00, v11, v22, v10, v20, v21, pad
 // Energy/virial sums over S without modifying it (en): raw sums -> out,
