@@ -51,6 +51,9 @@ struct Handle {
   double *d_gx = nullptr, *d_gw = nullptr, *d_gout = nullptr;
   int ccap = 0;
   double *d_cellp = nullptr;  // per-block partials of the cell adjoint
+  // pipelined de2 / potl: copy-in and copy-out streams, per-chunk events
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_copied[8] = {}, ev_gathered[8] = {};
   int last_n = 0;
   // pinned host buffers
   double *h_S = nullptr;
@@ -77,6 +80,12 @@ struct Handle {
 };
 
 Handle *H(void *p) { return reinterpret_cast<Handle *>(p); }
+
+// Pipelined de2 / potl: at most kPipeChunks chunks of at least kPipeMinChunk
+// points each.  Every chunk costs a handful of API calls on the host (copies,
+// events, a launch), which smaller chunks do not repay.
+constexpr int kPipeChunks = 4;
+constexpr int kPipeMinChunk = 131072;
 
 // Largest tabulated device Ewald influence function (A + 6 dA, FP64): a
 // table that stays in L2 is cheaper to read than the images are to evaluate;
@@ -239,6 +248,12 @@ void destroy(Handle *h) {
   for (auto &e : h->ev_stage)
     if (e) cudaEventDestroy(e);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  for (int c = 0; c < 8; c++) {
+    if (h->ev_copied[c]) cudaEventDestroy(h->ev_copied[c]);
+    if (h->ev_gathered[c]) cudaEventDestroy(h->ev_gathered[c]);
+  }
+  if (h->s_in) cudaStreamDestroy(h->s_in);
+  if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
 }
@@ -504,6 +519,32 @@ double de1(void *p, double vir[6]) {
   return r[0] * h->hcell.iV;
 }
 
+// True when p is host memory the GPU can copy asynchronously (pinned or
+// registered); pageable memory gets the single-copy path.
+static bool host_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Streams and events of the pipelined gather (created on first use).
+static bool ensure_pipeline(Handle *h) {
+  if (h->s_in) return true;
+  bool ok = CK(h, cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking)) &&
+            CK(h, cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+  for (int c = 0; c < kPipeChunks && ok; c++)
+    ok = CK(h, cudaEventCreateWithFlags(&h->ev_copied[c], cudaEventDisableTiming)) &&
+         CK(h, cudaEventCreateWithFlags(&h->ev_gathered[c], cudaEventDisableTiming));
+  return ok;
+}
+
+// de2 / potl (sfac.cpp:409-545) on host arrays.  With pinned host buffers
+// and enough points, the points are split into chunks: chunk c's copy in
+// (s_in), gather (the handle's stream) and copy out (s_out) overlap the
+// neighbouring chunks', so the two PCIe directions and the gather run at once.
 static void gather_call(Handle *h, int n, const double *w, const double *x, double *dx, double *phi) {
   if (h->state != 1) {
     printf("Error: You must call de1 before this routine.\n");
@@ -511,15 +552,46 @@ static void gather_call(Handle *h, int n, const double *w, const double *x, doub
   }
   if (n <= 0) return;
   if (!ensure_gather(h, n)) return;
-  if (!CK(h, cudaMemcpyAsync(h->d_gx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream))) return;
-  if (w && !CK(h, cudaMemcpyAsync(h->d_gw, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream))) return;
-  int k = launch_gather(h->geom, h->spline, n, h->d_gx, h->d_gw, h->d_real, dx ? h->d_gout : nullptr,
-                        phi ? h->d_gout : nullptr, h->stream);
+  double *out = dx ? dx : phi;
+  const int ow = dx ? 3 : 1;  // output words per point
+  const bool pipe = n >= 2 * kPipeMinChunk && host_pinned(x) && (!w || host_pinned(w)) && host_pinned(out) &&
+                    ensure_pipeline(h);
+  if (!pipe) {
+    if (!CK(h, cudaMemcpyAsync(h->d_gx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream))) return;
+    if (w && !CK(h, cudaMemcpyAsync(h->d_gw, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream))) return;
+    int k = launch_gather(h->geom, h->spline, n, h->d_gx, h->d_gw, h->d_real, dx ? h->d_gout : nullptr,
+                          phi ? h->d_gout : nullptr, h->stream);
+    if (!launched(h, k, "gather kernel")) return;
+    CK(h, cudaMemcpyAsync(out, h->d_gout, sizeof(double) * ow * n, cudaMemcpyDeviceToHost, h->stream));
+    sync(h);
+    return;
+  }
+  int nc = n / kPipeMinChunk;
+  if (nc > kPipeChunks) nc = kPipeChunks;
+  const int per = (n + nc - 1) / nc;
+  // copies in may start at once: the previous call on these buffers has
+  // completed (every call ends with a synchronisation)
+  int k = 0;
+  for (int c = 0; c < nc; c++) {
+    const int a0 = c * per, m = (a0 + per <= n) ? per : n - a0;
+    if (!CK(h, cudaMemcpyAsync(h->d_gx + 3L * a0, x + 3L * a0, sizeof(double) * 3 * m, cudaMemcpyHostToDevice,
+                               h->s_in)))
+      return;
+    if (w && !CK(h, cudaMemcpyAsync(h->d_gw + a0, w + a0, sizeof(double) * m, cudaMemcpyHostToDevice, h->s_in)))
+      return;
+    if (!CK(h, cudaEventRecord(h->ev_copied[c], h->s_in)) || !CK(h, cudaStreamWaitEvent(h->stream, h->ev_copied[c], 0)))
+      return;
+    k += launch_gather(h->geom, h->spline, m, h->d_gx + 3L * a0, h->d_gw + a0, h->d_real,
+                       dx ? h->d_gout + 3L * a0 : nullptr, phi ? h->d_gout + a0 : nullptr, h->stream);
+    if (!CK(h, cudaEventRecord(h->ev_gathered[c], h->stream)) ||
+        !CK(h, cudaStreamWaitEvent(h->s_out, h->ev_gathered[c], 0)))
+      return;
+    if (!CK(h, cudaMemcpyAsync(out + (long)ow * a0, h->d_gout + (long)ow * a0, sizeof(double) * ow * m,
+                               cudaMemcpyDeviceToHost, h->s_out)))
+      return;
+  }
   if (!launched(h, k, "gather kernel")) return;
-  if (dx)
-    CK(h, cudaMemcpyAsync(dx, h->d_gout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream));
-  else
-    CK(h, cudaMemcpyAsync(phi, h->d_gout, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->s_out));
   sync(h);
 }
 

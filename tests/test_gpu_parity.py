@@ -348,6 +348,36 @@ def test_gather_accepts_other_point_sets():
     assert rel_rms(out[0][1], out[1][1]) < 1e-5
 
 
+def test_pipelined_gather_matches_single_copy():
+    """de2/potl with pinned host arrays and enough points split the copies and
+    the gather into overlapping chunks; every point must come out exactly as
+    in the single-copy path taken for pageable arrays."""
+    import torch
+
+    c = configs.cfg2_water()
+    n = 400001  # several chunks, the last one short
+    rng = np.random.default_rng(11)
+    probes = rng.uniform(-1, 11, size=(n, 3))
+    pw = rng.normal(size=n)
+    s = E().Sfac(c.L, np.array(c.K), c.order)
+    s.set_ewald(c.beta, c.max_m)
+    s.sfac(c.q, c.x)
+    s.de1(np.zeros(6))
+    dx_pg, phi_pg = np.zeros((n, 3)), np.zeros(n)
+    s.de2(n, pw, probes, dx_pg)
+    s.potl(n, probes, phi_pg)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    xp, wp = pin(probes), pin(pw)
+    dx_pn, phi_pn = pin(np.zeros((n, 3))), pin(np.zeros(n))
+    for _ in range(2):
+        dx_pn[:] = 0.0
+        phi_pn[:] = 0.0
+        s.de2(n, wp, xp, dx_pn)
+        s.potl(n, xp, phi_pn)
+        np.testing.assert_array_equal(dx_pn, dx_pg)
+        np.testing.assert_array_equal(phi_pn, phi_pg)
+
+
 def test_deterministic_repeat():
     c = configs.cfg1_plain()
     a = solve("gpu", c.L, c.K, c.order, c.x, c.q, c.beta, c.max_m)
