@@ -10,15 +10,16 @@
 // four warps, lane (cx, cy) holds the 32 points of its (x, y) column in
 // registers.  The atoms of the brick's halo (the cells whose stencils reach
 // it) are found through the per-cell offsets of the sorted order; the warps
-// take them in round-robin chunks of 32: each lane stages one atom in shared
-// memory (cell offsets relative to the brick, the order-p B-spline weights
-// of its three fractions, the charge folded into the x weights).  The warp
-// then walks the staged atoms in order: each lane forms its column weight
-// wx*wy and adds wz[t] * (wx*wy) to the p registers the atom's z stencil
-// covers -- the z offset is the same for every lane, so it selects one
-// unrolled code path (a jump table), not a divergent branch.  Finally the
-// four partial bricks are summed in warp order through shared memory and
-// stored with lane = z (coalesced).
+// split them into equal contiguous shares, staged 32 at a time: each lane
+// stages one atom in shared memory (cell offsets relative to the brick, the
+// order-p B-spline weights of its three fractions, the charge folded into the
+// x weights, the z weights as a window aligned to 4).  The warp then walks
+// the staged atoms in order: each lane forms its column weight wx*wy and adds
+// it times the z window to the registers the window covers -- the window's
+// place is the same for every lane, so it selects one unrolled code path (a
+// jump table of ten), not a divergent branch.  Finally the four partial
+// bricks are summed in warp order through shared memory and stored with
+// lane = z (coalesced).
 #include "spme_kernels.hpp"
 
 namespace spme {
@@ -27,28 +28,34 @@ constexpr int SP_TX = 4, SP_TY = 8, SP_TZ = 32;
 constexpr int SP_WARPS = 4;
 
 // acc[Z + t] += w * wz[t] for the t with 0 <= Z + t < TZ (all compile-time).
-template <int P, int Z, int T = 0>
-__device__ __forceinline__ void add_at(float (&acc)[SP_TZ], float w, const float (&wz)[P]) {
-  if constexpr (T < P) {
-    if constexpr (Z + T >= 0 && Z + T < SP_TZ) acc[Z + T] = fmaf(w, wz[T], acc[Z + T]);
-    add_at<P, Z, T + 1>(acc, w, wz);
-  }
+// z weights of a staged atom as a window of NW floats starting at the
+// multiple of 4 at or below its first z offset rz (zero outside the P taps):
+// the window covers rz .. rz + P - 1 for P <= NW - 3.
+template <int P>
+struct ZWin {
+  static constexpr int NW = (P + 3 + 3) / 4 * 4;  // 8 for P <= 5, 12 for P <= 9
+  static constexpr int NV = NW / 4;                // float4 loads
+};
+
+// acc[4 G + t] += w * win[t] for the t with 0 <= 4 G + t < TZ (compile time).
+template <int NW, int G>
+__device__ __forceinline__ void add_win(float (&acc)[SP_TZ], float w, const float (&win)[NW]) {
+#pragma unroll
+  for (int t = 0; t < NW; t++)
+    if (4 * G + t >= 0 && 4 * G + t < SP_TZ) acc[4 * G + t] = fmaf(w, win[t], acc[4 * G + t]);
 }
 
-#define SP_CASE(Z) \
-  case Z:          \
-    add_at<P, Z>(acc, w, wz); \
+#define SP_CASE(G) \
+  case G:          \
+    add_win<NW, G>(acc, w, win); \
     break;
 
-// Dispatch on the warp-uniform stencil offset rz in [-(P-1), SP_TZ-1].
-template <int P>
-__device__ __forceinline__ void z_dispatch(int rz, float (&acc)[SP_TZ], float w, const float (&wz)[P]) {
-  switch (rz) {
-    SP_CASE(-7) SP_CASE(-6) SP_CASE(-5) SP_CASE(-4) SP_CASE(-3) SP_CASE(-2) SP_CASE(-1)
-    SP_CASE(0) SP_CASE(1) SP_CASE(2) SP_CASE(3) SP_CASE(4) SP_CASE(5) SP_CASE(6) SP_CASE(7)
-    SP_CASE(8) SP_CASE(9) SP_CASE(10) SP_CASE(11) SP_CASE(12) SP_CASE(13) SP_CASE(14) SP_CASE(15)
-    SP_CASE(16) SP_CASE(17) SP_CASE(18) SP_CASE(19) SP_CASE(20) SP_CASE(21) SP_CASE(22) SP_CASE(23)
-    SP_CASE(24) SP_CASE(25) SP_CASE(26) SP_CASE(27) SP_CASE(28) SP_CASE(29) SP_CASE(30) SP_CASE(31)
+// Dispatch on the warp-uniform window group g4 = floor(rz / 4) in [-2, 7]
+// (rz >= -(P-1) >= -7): ten code paths of NW fixed-register FMAs each.
+template <int NW>
+__device__ __forceinline__ void z_dispatch_win(int g4, float (&acc)[SP_TZ], float w, const float (&win)[NW]) {
+  switch (g4) {
+    SP_CASE(-2) SP_CASE(-1) SP_CASE(0) SP_CASE(1) SP_CASE(2) SP_CASE(3) SP_CASE(4) SP_CASE(5) SP_CASE(6) SP_CASE(7)
     default: break;
   }
 }
@@ -59,20 +66,22 @@ struct SpreadSmem {
   static constexpr int H = P / 2;
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
   // Staged atom, read by every lane in the walk:
-  //   zq: (rel bits, wz[0..P-1], pad) as float4s -- broadcast loads;
+  //   rel: rx | ry << 8 | (g4 + 64) << 16 (brick-relative row and window group);
+  //   zw: the z-weight window (ZWin) as float4s -- broadcast loads;
   //   wx: q*M(fx+i) at [3 + i], zero elsewhere, so lane cx reads [rx - cx + 3]
   //       with no range test (rx - cx in [-3, RX - 1]);
   //   wy: M(fy+j) at [7 + j], zero elsewhere, read at [ry - cy + 7].
   // The zero entries are written once per CTA; staging writes only the P
   // weights of each axis.  Odd row strides keep the lane-per-atom staging
   // stores free of bank conflicts.
-  static constexpr int NZ4 = (P + 1 + 3) / 4;
+  static constexpr int NZ4 = ZWin<P>::NV;
   static constexpr int WXS = (P + 6) | 1, WYS = (P + 14) | 1;
   int start[NR];                         // first sorted atom of each halo row segment
   int pref[NR + 1];                      // prefix sums of the row segment counts
   union {
     struct {
       float4 zq[SP_WARPS][32][NZ4];
+      int rel[SP_WARPS][32];
       float wx[SP_WARPS][32][WXS];
       float wy[SP_WARPS][32][WYS];
     } st;                                // staging (walk phase)
@@ -80,9 +89,9 @@ struct SpreadSmem {
   };
 };
 
-// One CTA per 4 x 8 x 32 brick; its 4 warps take the brick's staged atoms in
-// round-robin chunks of 32 and keep private register accumulators, summed in
-// warp order at the end (fixed order: deterministic).
+// One CTA per 4 x 8 x 32 brick; its 4 warps split the brick's atoms into
+// equal contiguous shares (staged 32 at a time) and keep private register
+// accumulators, summed in warp order at the end (fixed order: deterministic).
 template <int P>
 __global__ void __launch_bounds__(SP_WARPS * 32, 8) spread_reg_kernel(Geom g, Spline S, const int *__restrict__ cs,
                                                                   const uint32_t *__restrict__ keys,
@@ -141,9 +150,12 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 8) spread_reg_kernel(Geom g, Sp
     __syncthreads();
     const int total = s.pref[NR];
     const int zoff = ezs + H - (P - 1) - z0 - n2a;  // rz = n2 + zoff
-    for (int chunk = warp * 32; chunk < total; chunk += SP_WARPS * 32) {
+    // each warp takes an equal contiguous share of the segment's atoms,
+    // staged 32 at a time
+    const int w_lo = (int)((long)total * warp / SP_WARPS), w_hi = (int)((long)total * (warp + 1) / SP_WARPS);
+    for (int chunk = w_lo; chunk < w_hi; chunk += 32) {
       const int t = chunk + lane;
-      if (t < total) {
+      if (t < w_hi) {
         int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
@@ -155,37 +167,43 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 8) spread_reg_kernel(Geom g, Sp
         K2d.divmod(__ldg(keys + a), qk, n2);
         const int rx = lo / RY, ry = lo % RY;
         const int rz = (int)n2 + zoff;
-        float zw[4 * NZ4];
-        zw[0] = __int_as_float(rx | (ry << 8) | ((rz + 64) << 16));
+        const int g4 = rz >> 2;  // floor(rz / 4)
+        s.st.rel[warp][lane] = rx | (ry << 8) | ((g4 + 64) << 16);
+        float zt[P];
 #pragma unroll
         for (int i = 0; i < P; i++) {
           s.st.wx[warp][lane][3 + i] = u.w * bspl_eval(S, P, u.x, i);
           s.st.wy[warp][lane][7 + i] = bspl_eval(S, P, u.y, i);
-          zw[1 + i] = bspl_eval(S, P, u.z, P - 1 - i);
+          zt[i] = bspl_eval(S, P, u.z, P - 1 - i);  // weight of z = rz + i
+        }
+        const int sh = rz - 4 * g4;  // 0..3: first tap's place in the window
+        float zw[4 * NZ4];
+#pragma unroll
+        for (int t = 0; t < 4 * NZ4; t++) {
+          float v = 0.f;
+#pragma unroll
+          for (int i = 0; i < P; i++) v = (t == sh + i) ? zt[i] : v;
+          zw[t] = v;
         }
 #pragma unroll
-        for (int i = P + 1; i < 4 * NZ4; i++) zw[i] = 0.f;
-#pragma unroll
-        for (int v = 0; v < NZ4; v++) s.st.zq[warp][lane][v] = make_float4(zw[4 * v], zw[4 * v + 1], zw[4 * v + 2], zw[4 * v + 3]);
+        for (int v = 0; v < NZ4; v++)
+          s.st.zq[warp][lane][v] = make_float4(zw[4 * v], zw[4 * v + 1], zw[4 * v + 2], zw[4 * v + 3]);
       }
       __syncwarp();
-      const int na = min(32, total - chunk);
+      const int na = min(32, w_hi - chunk);
       const float *wxl = &s.st.wx[warp][0][3 - cx];
       const float *wyl = &s.st.wy[warp][0][7 - cy];
       for (int a = 0; a < na; a++) {
-        float zw[4 * NZ4];
+        float win[4 * NZ4];
 #pragma unroll
         for (int v = 0; v < NZ4; v++) {
           const float4 q = s.st.zq[warp][a][v];
-          zw[4 * v] = q.x; zw[4 * v + 1] = q.y; zw[4 * v + 2] = q.z; zw[4 * v + 3] = q.w;
+          win[4 * v] = q.x; win[4 * v + 1] = q.y; win[4 * v + 2] = q.z; win[4 * v + 3] = q.w;
         }
-        const int rel = __float_as_int(zw[0]);
-        const int rx = rel & 0xff, ry = (rel >> 8) & 0xff, rz = (rel >> 16) - 64;
+        const int rel = s.st.rel[warp][a];
+        const int rx = rel & 0xff, ry = (rel >> 8) & 0xff, g4 = (rel >> 16) - 64;
         const float w = wxl[a * SM::WXS + rx] * wyl[a * SM::WYS + ry];
-        float wz[P];
-#pragma unroll
-        for (int q = 0; q < P; q++) wz[q] = zw[1 + q];
-        z_dispatch<P>(rz, acc, w, wz);
+        z_dispatch_win<4 * NZ4>(g4, acc, w, win);
       }
       __syncwarp();
     }
