@@ -22,6 +22,7 @@ struct Handle {
   long nreal = 0, nmodes = 0, ncell = 0;
   Geom geom{};            // grid constants + device address of the box constants
   CellConst hcell{};      // host copy of the current box constants
+  double L[6] = {0, 0, 0, 0, 0, 0};  // current box [ax, by, cz, bx, cx, cy]
   CellConst *d_cell = nullptr;
   InfConst hic{};         // host copy of the device Ewald constants
   InfConst *d_ic = nullptr;
@@ -51,6 +52,14 @@ struct Handle {
   double *d_gx = nullptr, *d_gw = nullptr, *d_gout = nullptr;
   int ccap = 0;
   double *d_cellp = nullptr;  // per-block partials of the cell adjoint
+  // real-space term: coarse cell sort and per-point records
+  struct RealBufs {
+    SortBuffers sb{};
+    int cap = 0;
+    long ncell = 0;
+    double4 *rec = nullptr;
+    double *x = nullptr, *w = nullptr, *dx = nullptr, *part = nullptr, *out = nullptr;
+  } rs;
   // pipelined de2 / potl: copy-in and copy-out streams, per-chunk events
   cudaStream_t s_in = nullptr, s_out = nullptr;
   cudaEvent_t ev_copied[8] = {}, ev_gathered[8] = {};
@@ -125,6 +134,7 @@ bool check(Handle *h, cudaError_t e, const char *what);
 // stream (ordered before any later solve; kernel arguments do not change, so
 // captured graphs stay valid).
 bool set_cell(Handle *h, const double L[6]) {
+  for (int i = 0; i < 6; i++) h->L[i] = L[i];
   h->hcell = make_cell(L);
   return check(h, cudaMemcpyAsync(h->d_cell, &h->hcell, sizeof(CellConst), cudaMemcpyHostToDevice, h->stream),
                "set_cell copy");
@@ -158,6 +168,48 @@ void make_spline(int n, Spline &S, SplineNodes &nodes) {
       S.c[j * n + i] = (float)c;
       if (i == n - 1) nodes.Mj[j] = (double)c;  // constant term: M_n(j)
     }
+}
+
+void free_real(Handle *h) {
+  Handle::RealBufs &r = h->rs;
+  for (int i = 0; i < 2; i++) {
+    dfree(r.sb.keys[i]);
+    dfree(r.sb.vals[i]);
+  }
+  dfree(r.sb.tmp);
+  dfree(r.sb.rec);
+  dfree(r.sb.rec_sorted);
+  dfree(r.sb.hist);
+  dfree(r.sb.cell_start);
+  dfree(r.rec);
+  dfree(r.x);
+  dfree(r.w);
+  dfree(r.dx);
+  dfree(r.part);
+  dfree(r.out);
+  r.cap = 0;
+  r.ncell = 0;
+}
+
+// Buffers of the real-space term for n points on a coarse grid of ncell cells.
+bool ensure_real(Handle *h, int n, long ncell) {
+  Handle::RealBufs &r = h->rs;
+  if (n <= r.cap && ncell == r.ncell && r.out) return true;
+  const int cap = n > r.cap ? n + n / 2 + 64 : r.cap;
+  free_real(h);
+  bool ok = true;
+  for (int i = 0; i < 2 && ok; i++) ok = dalloc(h, &r.sb.keys[i], cap) && dalloc(h, &r.sb.vals[i], cap);
+  ok = ok && dalloc(h, &r.sb.tmp, cap) && dalloc(h, &r.sb.rec, cap) && dalloc(h, &r.sb.rec_sorted, cap) &&
+       dalloc(h, &r.sb.hist, cap) && dalloc(h, &r.sb.cell_start, cell_count_words(ncell)) &&
+       dalloc(h, &r.rec, cap) && dalloc(h, &r.x, 3 * (size_t)cap) && dalloc(h, &r.w, cap) &&
+       dalloc(h, &r.dx, 3 * (size_t)cap) && dalloc(h, &r.part, real_partial_words(cap)) && dalloc(h, &r.out, 16);
+  if (!ok) {
+    free_real(h);
+    return false;
+  }
+  r.cap = cap;
+  r.ncell = ncell;
+  return true;
 }
 
 void free_atoms(Handle *h) {
@@ -252,6 +304,7 @@ void destroy(Handle *h) {
     if (h->ev_copied[c]) cudaEventDestroy(h->ev_copied[c]);
     if (h->ev_gathered[c]) cudaEventDestroy(h->ev_gathered[c]);
   }
+  free_real(h);
   if (h->s_in) cudaStreamDestroy(h->s_in);
   if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -605,6 +658,76 @@ void potl(void *p, int n, const double *x, double *phi) {
   Handle *h = H(p);
   if (!h) return;
   gather_call(h, n, nullptr, x, nullptr, phi);
+}
+
+// Coarse grid of the real-space cell list: cells at least rcut wide along
+// every fractional axis (perpendicular widths of the box from iL).  False when
+// rcut exceeds half the smallest width (the minimum image would not be unique).
+static bool real_grid(const Handle *h, double rcut, int nb[3]) {
+  const CellConst &c = h->hcell;
+  const double wd[3] = {1.0 / sqrt(c.iL00 * c.iL00 + c.iL10 * c.iL10 + c.iL20 * c.iL20),
+                        1.0 / sqrt(c.iL11 * c.iL11 + c.iL21 * c.iL21), 1.0 / fabs(c.iL22)};
+  const double wmin = fmin(wd[0], fmin(wd[1], wd[2]));
+  if (!(rcut > 0.0) || rcut > 0.5 * wmin) return false;
+  for (int d = 0; d < 3; d++) {
+    const double m = floor(wd[d] / rcut);
+    nb[d] = m < 1.0 ? 1 : (m > 512.0 ? 512 : (int)m);
+  }
+  return true;
+}
+
+// Checks the arguments and sizes the buffers; fills the coarse geometry.
+static int real_prepare(Handle *h, int n, double eta, double rcut, Geom &cg) {
+  int nb[3];
+  if (n < 0 || !(eta > 0.0)) {
+    printf("sfac_real_space: bad atom count %d or eta %g\n", n, eta);
+    return 1;
+  }
+  if (!real_grid(h, rcut, nb)) {
+    printf("sfac_real_space: cutoff %g must be positive and at most half the smallest box width\n", rcut);
+    return 1;
+  }
+  if (!ensure_real(h, n, (long)nb[0] * nb[1] * nb[2])) return 2;
+  cg = Geom{};
+  cg.K0 = nb[0];
+  cg.K1 = nb[1];
+  cg.K2 = nb[2];
+  cg.ldim = nb[2] / 2 + 1;
+  cg.order = h->order;
+  cg.cell = h->d_cell;
+  return 0;
+}
+
+int sfac_real_space_device(void *p, int n, const double *x, const double *w, double eta, double rcut, double *out,
+                           double *dx) {
+  Handle *h = H(p);
+  if (!h || !out || (n > 0 && (!x || !w))) return 1;
+  Geom cg;
+  const int rc = real_prepare(h, n, eta, rcut, cg);
+  if (rc) return rc;
+  const int k = launch_real_space(cg, h->L, n, x, w, (float)eta, (float)rcut, h->rs.sb, h->rs.rec, dx, h->rs.part,
+                                  eta, out, h->stream);
+  return launched(h, k, "real-space kernels") ? 0 : 2;
+}
+
+int sfac_real_space(void *p, int n, const double *w, const double *x, double eta, double rcut, double out[10],
+                    double *dx) {
+  Handle *h = H(p);
+  if (!h || !out || (n > 0 && (!x || !w))) return 1;
+  Geom cg;
+  const int rc = real_prepare(h, n, eta, rcut, cg);
+  if (rc) return rc;
+  if (n > 0 && (!CK(h, cudaMemcpyAsync(h->rs.x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream)) ||
+                !CK(h, cudaMemcpyAsync(h->rs.w, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream))))
+    return 2;
+  const int k = launch_real_space(cg, h->L, n, h->rs.x, h->rs.w, (float)eta, (float)rcut, h->rs.sb, h->rs.rec,
+                                  dx ? h->rs.dx : nullptr, h->rs.part, eta, h->rs.out, h->stream);
+  if (!launched(h, k, "real-space kernels")) return 2;
+  if (!CK(h, cudaMemcpyAsync(out, h->rs.out, sizeof(double) * 10, cudaMemcpyDeviceToHost, h->stream))) return 2;
+  if (dx && n > 0 &&
+      !CK(h, cudaMemcpyAsync(dx, h->rs.dx, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream)))
+    return 2;
+  return sync(h) ? 0 : 2;
 }
 
 int sfac_set_ewald(void *p, double beta, double max_m) {

@@ -139,4 +139,14 @@ int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, c
                        const float4 *rec = nullptr);
 size_t gather_cell_words(int cap);
 
+// ---- real-space term (k_real.cu) ----
+// Cell sort of the points on the coarse grid `coarse` (cells >= rcut wide),
+// then the minimum-image erfc pair sum: dx (n x 3, input order, may be null)
+// and out (device, 10 doubles: E_real, E_self, E_net, virial[6], net-charge
+// virial diagonal).  partials: real_partial_words(n) doubles.
+int launch_real_space(const Geom &coarse, const double L[6], int n, const double *x, const double *w, float eta,
+                      float rcut, SortBuffers &sb, double4 *rec, double *dx, double *partials, double eta_d,
+                      double *out, cudaStream_t st);
+size_t real_partial_words(int cap);
+
 }  // namespace spme

@@ -72,6 +72,7 @@ def describe_sfac():
     decl(lib.sfac_error_string, c_char_p, sfac_p)
     decl(lib.sfac_device, c_int, sfac_p)
     decl(lib.sfac_kernel_launches, c_longlong, sfac_p)
+    decl(lib.sfac_real_space, c_int, sfac_p, c_int, nparr, nparr, c_double, c_double, nparr_t(10), c_void_p)
     intarr = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     decl(lib.sfac_debug_sort, c_int, sfac_p, c_int, intarr, intarr)
     decl(lib.sfac_debug_spread, c_int, sfac_p,
@@ -153,6 +154,27 @@ class Sfac:
             self.set_A(self.f, 1.0)
         elif hasattr(self, "_ewald"):
             self.set_ewald(*self._ewald)
+
+    def real_space(self, w, x, eta, rcut, grad=True):
+        """Real-space Ewald term beside this solver's reciprocal sum (an
+        addition: the reference's notes give only the self correction,
+        notes.tex:73-77).  Returns (E_real, E_self, E_net, vir[6], dx): with
+        the Ewald influence function of the same eta, en() + E_real +
+        E_self + E_net is the full Ewald energy; vir is E_real's virial in
+        de1's convention plus the net-charge term on its diagonal; dx is
+        dE_real/dx (n x 3) or None."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = len(w)
+        out = np.zeros(10)
+        dx = np.zeros((n, 3)) if grad else None
+        rc = self._libsfac.sfac_real_space(self._data, n, w, x, float(eta), float(rcut), out,
+                                           dx.ctypes.data if grad else None)
+        if rc != 0:
+            raise RuntimeError("sfac_real_space failed (%d)" % rc)
+        vir = out[3:9].copy()
+        vir[:3] += out[9]
+        return out[0], out[1], out[2], vir, dx
 
     # diagnostics (additions)
     def last_error(self):

@@ -84,6 +84,27 @@ void potl(void *sfac, int n, const double *x, double *phi);
  * set_A).  Returns 0. */
 int sfac_set_ewald(void *sfac, double beta, double max_m);
 
+/* Real-space Ewald term and corrections beside the reciprocal sum: with the
+ * Ewald influence function of splitting parameter eta (sfac_set_ewald, or
+ * ewald.py's ewald_f), E_recip + out[0] + out[1] + out[2] is the full Ewald
+ * energy (CGS) and does not depend on eta (notes.tex:68-79 gives E_self;
+ * E_real is the erfc complement of f, E_net the neutralising background).
+ *   out[0] E_real = 1/2 sum_{i != j, r < rcut} q_i q_j erfc(eta r) / r
+ *          (minimum image; rcut <= half the smallest box width),
+ *   out[1] E_self = -eta/sqrt(pi) sum q^2,
+ *   out[2] E_net  = -pi (sum q)^2 / (2 V eta^2),
+ *   out[3..8] virial of E_real in de1's convention ([xx,yy,zz,yx,zx,zy]),
+ *   out[9] virial of E_net (add to xx, yy and zz).
+ * dx (n x 3, may be null): dE_real/dx.  Host arrays; uses the handle's
+ * current box.  Returns 0, 1 on bad arguments, 2 on a CUDA error.
+ * No counterpart in the reference (its notes give the correction only). */
+int sfac_real_space(void *sfac, int n, const double *w, const double *x, double eta, double rcut, double out[10],
+                    double *dx);
+/* The same on device arrays (out: 10 device doubles), enqueued on the
+ * handle's stream without synchronising. */
+int sfac_real_space_device(void *sfac, int n, const double *x, const double *w, double eta, double rcut, double *out,
+                           double *dx);
+
 /* Last CUDA or argument error seen by this handle (0 = none), and its text. */
 int sfac_last_error(void *sfac);
 const char *sfac_error_string(void *sfac);

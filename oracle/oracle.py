@@ -247,3 +247,54 @@ def LofS(L):
 def SofL(L):
     """6-vector from the box matrix (ewald.py:139-140)."""
     return np.array([L[0, 0], L[1, 1], L[2, 2], L[1, 0], L[2, 0], L[2, 1]])
+
+
+def real_space(L, x, q, eta, rcut):
+    """FP64 restatement of the real-space Ewald term and its corrections, all
+    pairs (O(N^2), small systems only), minimum image.  With the reference's
+    influence function f(z) = exp(-z pi^2/eta^2)/(pi z) (ewald.py:124-132)
+    the reciprocal sum is the erfc-split long-range part of the CGS Coulomb
+    energy, so (notes.tex:68-79, E_self being the "correction energy" there):
+      E_real = 1/2 sum_{i != j, r < rcut} q_i q_j erfc(eta r)/r,
+      E_self = -eta/sqrt(pi) sum q^2,
+      E_net  = -pi (sum q)^2 / (2 V eta^2)  (the "further corrections ... if
+               sum q != 0" the notes mention: a neutralising background).
+    Returns (E_real, E_self, E_net, vir[6], dx) with vir = -W/V,
+    W = sum_pairs q q phi'(r)/r r r^T, in de1's [xx, yy, zz, yx, zx, zy]
+    order plus the background's -pi Q^2/(2 eta^2 V^2) on the diagonal, and dx
+    = dE_real/dx."""
+    from scipy.special import erfc
+
+    Lm = LofS(L)
+    V = L[0] * L[1] * L[2]
+    iLt = np.linalg.inv(Lm)  # s = x @ iLt
+    x = np.asarray(x, dtype=np.float64)
+    q = np.asarray(q, dtype=np.float64)
+    s = x @ iLt
+    n = len(q)
+    e = 0.0
+    W = np.zeros((3, 3))
+    dx = np.zeros((n, 3))
+    for i in range(n):
+        ds = s - s[i]
+        ds -= np.rint(ds)
+        d = ds @ Lm  # r_j - r_i
+        r2 = np.einsum("ij,ij->i", d, d)
+        mask = (r2 < rcut * rcut) & (np.arange(n) != i)
+        if not mask.any():
+            continue
+        r = np.sqrt(r2[mask])
+        dd = d[mask]
+        qq = q[i] * q[mask]
+        phi = erfc(eta * r) / r
+        dphi = -(2.0 * eta / np.sqrt(np.pi) * np.exp(-(eta * r) ** 2) + phi) / r
+        e += 0.5 * np.sum(qq * phi)
+        t = qq * dphi / r
+        dx[i] = -np.sum(t[:, None] * dd, axis=0)
+        W += 0.5 * np.einsum("k,ka,kb->ab", t, dd, dd)
+    Q = q.sum()
+    e_self = -eta / np.sqrt(np.pi) * np.sum(q * q)
+    e_net = -np.pi * Q * Q / (2.0 * V * eta * eta)
+    vir = SofL(W) / -V
+    vir[:3] += -np.pi * Q * Q / (2.0 * eta * eta * V * V)
+    return e, e_self, e_net, vir, dx

@@ -1,0 +1,111 @@
+"""Real-space Ewald term (sfac_real_space): parity with the FP64 oracle and
+the physical check that the full Ewald energy does not depend on the
+splitting parameter eta (notes.tex:68-79)."""
+import numpy as np
+import pytest
+
+from ewaldcorrel_b200 import configs
+from oracle import oracle as O
+from tests.spme_testlib import rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _libs(libsfac_path, oracle_built):
+    return libsfac_path
+
+
+def E():
+    from ewaldcorrel_b200 import ewald
+
+    return ewald
+
+
+def _check(g, o, name):
+    e, es, en, vir, dx = g
+    oe, oes, oen, ovir, odx = o
+    assert abs(e - oe) <= 1e-6 * abs(oe), f"{name}: E_real {e!r} vs {oe!r}"
+    assert abs(es - oes) <= 1e-12 * abs(oes), f"{name}: E_self"
+    assert abs(en - oen) <= 1e-12 * max(abs(oen), 1e-300) + 1e-12, f"{name}: E_net"
+    assert np.abs(vir - ovir).max() <= 1e-5 * np.abs(ovir).max(), f"{name}: virial"
+    assert rel_rms(dx, odx) <= 1e-5, f"{name}: dE/dx"
+
+
+def test_real_space_matches_oracle_cubic():
+    c = configs.cfg1_plain()
+    s = E().Sfac(c.L, np.array(c.K), c.order)
+    g = s.real_space(c.q, c.x, c.beta, 1.45)
+    o = O.real_space(c.L, c.x, c.q, c.beta, 1.45)
+    _check(g, o, "cfg1")
+
+
+def test_real_space_matches_oracle_triclinic_charged():
+    rng = np.random.default_rng(21)
+    L = np.array([4.0, 3.6, 3.8, 0.9, -0.7, 0.5])
+    n = 700
+    x = rng.uniform(0, 1, size=(n, 3)) @ O.LofS(L) + rng.normal(0, 2.0, size=(n, 3))  # unwrapped positions
+    q = rng.normal(size=n)  # not neutral: exercises the background term
+    s = E().Sfac(L, np.array([24, 24, 24]), 4)
+    g = s.real_space(q, x, 2.9, 1.7)
+    o = O.real_space(L, x, q, 2.9, 1.7)
+    _check(g, o, "triclinic")
+
+
+def test_real_space_rejects_long_cutoff():
+    c = configs.cfg1_plain()
+    s = E().Sfac(c.L, np.array(c.K), c.order)
+    with pytest.raises(RuntimeError):
+        s.real_space(c.q, c.x, c.beta, 1.6)  # more than half the 3 nm box
+
+
+def _total(L, K, order, x, q, eta, rcut):
+    s = E().Sfac(L, np.array(K), order)
+    s.set_ewald(eta, eta * np.sqrt(np.log(1e16)) / np.pi)
+    s.sfac(q, x)
+    vir = np.zeros(6)
+    e_rec = s.de1(vir)
+    n = len(q)
+    dx = np.zeros((n, 3))
+    s.de2(n, q, x, dx)
+    e_real, e_self, e_net, vir_real, dx_real = s.real_space(q, x, eta, rcut)
+    return e_rec + e_real + e_self + e_net, dx + dx_real, vir + vir_real, (e_rec, e_real, e_self)
+
+
+def test_total_ewald_energy_independent_of_eta():
+    """E_recip + E_real + E_self: each term moves by O(1) between the two
+    splittings, their sum (the Coulomb energy of the periodic system) not."""
+    c = configs.cfg1_plain()
+    K, order, rcut = (64, 64, 64), 8, 1.45
+    ea, fa, va, parts_a = _total(c.L, K, order, c.x, c.q, 3.9, rcut)
+    eb, fb, vb, parts_b = _total(c.L, K, order, c.x, c.q, 4.6, rcut)
+    assert abs(parts_a[0] - parts_b[0]) > 1e-2 * abs(ea)  # the split really moved
+    assert abs(ea - eb) <= 2e-6 * abs(ea), (ea, eb, parts_a, parts_b)
+    assert rel_rms(fa, fb) <= 2e-5
+    assert np.abs(va - vb).max() <= 2e-5 * np.abs(va).max()
+
+
+def test_real_space_device_entry_matches_host():
+    import torch
+
+    c = configs.cfg1_plain()
+    s = E().Sfac(c.L, np.array(c.K), c.order)
+    host = s.real_space(c.q, c.x, c.beta, 1.45)
+    lib = s._libsfac
+    import ctypes
+
+    lib.sfac_real_space_device.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 2 + \
+        [ctypes.c_double, ctypes.c_double] + [ctypes.c_void_p] * 2
+    lib.sfac_real_space_device.restype = ctypes.c_int
+    dev = torch.device("cuda", lib.sfac_device(s._data))
+    x = torch.from_numpy(c.x).to(dev)
+    q = torch.from_numpy(c.q).to(dev)
+    out = torch.zeros(10, dtype=torch.float64, device=dev)
+    dx = torch.zeros((c.n, 3), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    assert lib.sfac_real_space_device(s._data, c.n, x.data_ptr(), q.data_ptr(), c.beta, 1.45, out.data_ptr(),
+                                      dx.data_ptr()) == 0
+    torch.cuda.synchronize(dev)
+    o = out.cpu().numpy()
+    assert o[0] == host[0] and o[1] == host[1]
+    np.testing.assert_array_equal(dx.cpu().numpy(), host[4])
