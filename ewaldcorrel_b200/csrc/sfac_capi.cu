@@ -52,6 +52,11 @@ struct Handle {
   double *d_gx = nullptr, *d_gw = nullptr, *d_gout = nullptr;
   int ccap = 0;
   double *d_cellp = nullptr;  // per-block partials of the cell adjoint
+  // structure-factor analysis: sum of |S|^2 over frames, radial binning scratch
+  double *d_sk = nullptr;
+  long long sk_frames = 0;
+  double *d_skpart = nullptr, *d_skres = nullptr;
+  int sk_cap = 0;
   // real-space term: coarse cell sort and per-point records
   struct RealBufs {
     SortBuffers sb{};
@@ -305,6 +310,9 @@ void destroy(Handle *h) {
     if (h->ev_gathered[c]) cudaEventDestroy(h->ev_gathered[c]);
   }
   free_real(h);
+  dfree(h->d_sk);
+  dfree(h->d_skpart);
+  dfree(h->d_skres);
   if (h->s_in) cudaStreamDestroy(h->s_in);
   if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -726,6 +734,59 @@ int sfac_real_space(void *p, int n, const double *w, const double *x, double eta
   if (!CK(h, cudaMemcpyAsync(out, h->rs.out, sizeof(double) * 10, cudaMemcpyDeviceToHost, h->stream))) return 2;
   if (dx && n > 0 &&
       !CK(h, cudaMemcpyAsync(dx, h->rs.dx, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, h->stream)))
+    return 2;
+  return sync(h) ? 0 : 2;
+}
+
+int sfac_sk_reset(void *p) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (!h->d_sk && !dalloc(h, &h->d_sk, (size_t)h->nmodes)) return 2;
+  h->sk_frames = 0;
+  return CK(h, cudaMemsetAsync(h->d_sk, 0, sizeof(double) * h->nmodes, h->stream)) ? 0 : 2;
+}
+
+int sfac_sk_accumulate(void *p) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (h->state != 0) {
+    printf("Error: You must call sfac before this routine.\n");
+    return 1;
+  }
+  if (!h->d_sk && sfac_sk_reset(p) != 0) return 2;
+  const int k = launch_sk_accumulate(h->nmodes, h->d_cplx, h->d_sk, h->stream);
+  if (!launched(h, k, "sk accumulate")) return 2;
+  h->sk_frames++;
+  return 0;
+}
+
+int sfac_sk_get(void *p, double *out, long long *frames) {
+  Handle *h = H(p);
+  if (!h || !out) return 1;
+  if (!h->d_sk && sfac_sk_reset(p) != 0) return 2;
+  if (frames) *frames = h->sk_frames;
+  if (!CK(h, cudaMemcpyAsync(out, h->d_sk, sizeof(double) * h->nmodes, cudaMemcpyDeviceToHost, h->stream))) return 2;
+  return sync(h) ? 0 : 2;
+}
+
+int sfac_sk_radial(void *p, int nbins, double kmax, double *sums, double *counts) {
+  Handle *h = H(p);
+  if (!h || !sums || !counts || nbins < 1 || !(kmax > 0.0)) return 1;
+  if (!h->d_sk && sfac_sk_reset(p) != 0) return 2;
+  if (nbins > h->sk_cap || !h->d_skpart) {
+    dfree(h->d_skpart);
+    dfree(h->d_skres);
+    if (!dalloc(h, &h->d_skpart, sk_partial_words()) || !dalloc(h, &h->d_skres, 2 * (size_t)nbins)) {
+      h->sk_cap = 0;
+      return 2;
+    }
+    h->sk_cap = nbins;
+  }
+  const int k = launch_sk_radial(h->geom, h->d_sk, nbins, kmax / nbins, h->d_skpart, h->d_skres, h->d_skres + nbins,
+                                 h->stream);
+  if (!launched(h, k, "sk radial")) return 2;
+  if (!CK(h, cudaMemcpyAsync(sums, h->d_skres, sizeof(double) * nbins, cudaMemcpyDeviceToHost, h->stream)) ||
+      !CK(h, cudaMemcpyAsync(counts, h->d_skres + nbins, sizeof(double) * nbins, cudaMemcpyDeviceToHost, h->stream)))
     return 2;
   return sync(h) ? 0 : 2;
 }

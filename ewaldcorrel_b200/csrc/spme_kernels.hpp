@@ -139,6 +139,12 @@ int launch_gather_cell(const Geom &g, const Spline &S, int n, const double *x, c
                        const float4 *rec = nullptr);
 size_t gather_cell_words(int cap);
 
+// ---- structure-factor analysis (k_sk.cu) ----
+int launch_sk_accumulate(long nmodes, const float2 *S, double *acc, cudaStream_t st);
+size_t sk_partial_words();
+int launch_sk_radial(const Geom &g, const double *acc, int nbins, double dk, double *partials, double *sums,
+                     double *counts, cudaStream_t st);
+
 // ---- real-space term (k_real.cu) ----
 // Cell sort of the points on the coarse grid `coarse` (cells >= rcut wide),
 // then the minimum-image erfc pair sum: dx (n x 3, input order, may be null)

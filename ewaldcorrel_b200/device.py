@@ -33,6 +33,9 @@ def _lib():
         lib.sfac_solve_device_timed.restype = c_int
         lib.sfac_set_graphs.argtypes = [c_void_p, c_int]
         lib.sfac_set_graphs.restype = c_int
+        lib.sfac_real_space_device.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_void_p,
+                                               c_void_p]
+        lib.sfac_real_space_device.restype = c_int
         lib._device_declared = True
     return lib
 
@@ -101,3 +104,18 @@ class SpmeSolver:
         if rc != 0:
             raise RuntimeError(f"sfac_solve_device_timed failed ({rc}): {self.sf.last_error()}")
         return dict(zip(STAGES, [float(v) for v in ms]))
+
+    def real_space(self, x, q, eta, rcut, out=None, dx=None):
+        """Enqueues the real-space Ewald term (sfac_real_space_device): out
+        (10 doubles on device) = [E_real, E_self, E_net, virial[6], net-charge
+        virial diagonal]; dx (n x 3, may be None) = dE_real/dx."""
+        t = self.torch
+        n = q.shape[0]
+        if out is None:
+            out = t.empty(10, dtype=t.float64, device=self.device)
+        self._check(x, q, dx, None, None)
+        rc = self.lib.sfac_real_space_device(self.handle, n, _ptr(x), _ptr(q), float(eta), float(rcut), _ptr(out),
+                                             _ptr(dx))
+        if rc != 0:
+            raise RuntimeError(f"sfac_real_space_device failed ({rc}): {self.sf.last_error()}")
+        return out

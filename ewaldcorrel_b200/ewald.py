@@ -14,7 +14,7 @@ handle's diagnostics.
 from __future__ import annotations
 
 import os
-from ctypes import CDLL, POINTER, PYFUNCTYPE, c_char_p, c_double, c_int, c_longlong, c_void_p, cast
+from ctypes import CDLL, POINTER, PYFUNCTYPE, byref, c_char_p, c_double, c_int, c_longlong, c_void_p, cast
 from math import exp, pi
 
 import numpy as np
@@ -73,6 +73,10 @@ def describe_sfac():
     decl(lib.sfac_device, c_int, sfac_p)
     decl(lib.sfac_kernel_launches, c_longlong, sfac_p)
     decl(lib.sfac_real_space, c_int, sfac_p, c_int, nparr, nparr, c_double, c_double, nparr_t(10), c_void_p)
+    decl(lib.sfac_sk_reset, c_int, sfac_p)
+    decl(lib.sfac_sk_accumulate, c_int, sfac_p)
+    decl(lib.sfac_sk_get, c_int, sfac_p, nparr, POINTER(c_longlong))
+    decl(lib.sfac_sk_radial, c_int, sfac_p, c_int, c_double, nparr, nparr)
     intarr = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     decl(lib.sfac_debug_sort, c_int, sfac_p, c_int, intarr, intarr)
     decl(lib.sfac_debug_spread, c_int, sfac_p,
@@ -175,6 +179,32 @@ class Sfac:
         vir = out[3:9].copy()
         vir[:3] += out[9]
         return out[0], out[1], out[2], vir, dx
+
+    # structure-factor analysis (additions; run.py:27-47, plot.py:9-32)
+    def sk_reset(self):
+        if self._libsfac.sfac_sk_reset(self._data) != 0:
+            raise RuntimeError("sfac_sk_reset failed")
+
+    def sk_accumulate(self):
+        """Adds |S|^2 of the last sfac() to the running sum."""
+        if self._libsfac.sfac_sk_accumulate(self._data) != 0:
+            raise RuntimeError("sfac_sk_accumulate failed (call sfac first)")
+
+    def sk_get(self):
+        """(sum of |S|^2 as a (K0, K1, ldim) array, number of frames)."""
+        out = np.zeros((self.K[0], self.K[1], self.ldim))
+        frames = c_longlong(0)
+        if self._libsfac.sfac_sk_get(self._data, out, byref(frames)) != 0:
+            raise RuntimeError("sfac_sk_get failed")
+        return out, int(frames.value)
+
+    def sk_radial(self, nbins, kmax):
+        """(bin sums, bin counts) of the accumulated |S|^2 over |k| = 2 pi |m|
+        in nbins bins of width kmax / nbins."""
+        sums, counts = np.zeros(int(nbins)), np.zeros(int(nbins))
+        if self._libsfac.sfac_sk_radial(self._data, int(nbins), float(kmax), sums, counts) != 0:
+            raise RuntimeError("sfac_sk_radial failed")
+        return sums, counts
 
     # diagnostics (additions)
     def last_error(self):

@@ -84,6 +84,24 @@ void potl(void *sfac, int n, const double *x, double *phi);
  * set_A).  Returns 0. */
 int sfac_set_ewald(void *sfac, double beta, double max_m);
 
+/* Structure-factor analysis over frames, on the device: what the
+ * reference's run.py:27-47 does on the host (Q += |get_S()|^2 per frame) and
+ * plot.py:9-32's radial binning.  No counterpart in the reference's library.
+ *   sfac_sk_reset       zeroes the sum of |S|^2 and the frame count;
+ *   sfac_sk_accumulate  after sfac: adds |S(m)|^2 of every stored mode (FP64);
+ *   sfac_sk_get         copies the sum (K0 x K1 x ldim doubles, get_S's
+ *                       mode order) and the frame count;
+ *   sfac_sk_radial      sums and counts of the stored modes in nbins bins of
+ *                       |k| = 2 pi |m| (m the reciprocal vector of the
+ *                       signed x/y indices and the stored z index, m . x =
+ *                       n . s in the current box), width kmax/nbins; modes
+ *                       beyond kmax are left out.
+ * Return 0, 1 on bad arguments or state, 2 on a CUDA error. */
+int sfac_sk_reset(void *sfac);
+int sfac_sk_accumulate(void *sfac);
+int sfac_sk_get(void *sfac, double *out, long long *frames);
+int sfac_sk_radial(void *sfac, int nbins, double kmax, double *sums, double *counts);
+
 /* Real-space Ewald term and corrections beside the reciprocal sum: with the
  * Ewald influence function of splitting parameter eta (sfac_set_ewald, or
  * ewald.py's ewald_f), E_recip + out[0] + out[1] + out[2] is the full Ewald

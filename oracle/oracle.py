@@ -298,3 +298,32 @@ def real_space(L, x, q, eta, rcut):
     vir = SofL(W) / -V
     vir[:3] += -np.pi * Q * Q / (2.0 * eta * eta * V * V)
     return e, e_self, e_net, vir, dx
+
+
+def sk_radial(L, K, acc, nbins, kmax):
+    """FP64 restatement of the radial binning of a sum of |S|^2 over the
+    stored half-space modes (the reference's plot.py:9-32, on the general
+    box): |k| = 2 pi |m|, m = iL^T n with n the signed x/y frequency indices
+    and the stored z index; bin floor(|k| / dk), dk = kmax / nbins; returns
+    per-bin (sums, counts).  plot.py folds the stored z index as if that axis
+    had ldim points (index >= ldim/2 taken as negative); this restatement, like
+    the device code, uses the stored z index as it is."""
+    K0, K1, K2 = K
+    ldim = K2 // 2 + 1
+    n0 = np.arange(K0)
+    n0 = np.where(n0 > K0 // 2, n0 - K0, n0).astype(np.float64)
+    n1 = np.arange(K1)
+    n1 = np.where(n1 > K1 // 2, n1 - K1, n1).astype(np.float64)
+    n2 = np.arange(ldim).astype(np.float64)
+    N0, N1, N2 = np.meshgrid(n0, n1, n2, indexing="ij")
+    # m . x = n . s with s = x @ inv(box), box rows a, b, c: m = inv(box) n
+    # (set_A's mx, my, mz, sfac.cpp:240-262)
+    iL = np.linalg.inv(LofS(L))
+    M = np.stack([N0, N1, N2], axis=-1) @ iL.T
+    k = 2.0 * np.pi * np.sqrt(np.sum(M * M, axis=-1))
+    b = np.floor(k / (kmax / nbins)).astype(np.int64).ravel()
+    v = np.asarray(acc, dtype=np.float64).ravel()
+    keep = (b >= 0) & (b < nbins)
+    sums = np.bincount(b[keep], weights=v[keep], minlength=nbins)
+    counts = np.bincount(b[keep], minlength=nbins).astype(np.float64)
+    return sums, counts
