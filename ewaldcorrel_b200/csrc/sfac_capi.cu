@@ -668,7 +668,7 @@ void potl(void *p, int n, const double *x, double *phi) {
   gather_call(h, n, nullptr, x, nullptr, phi);
 }
 
-// Coarse grid of the real-space cell list: cells at least rcut wide along
+// Coarse grid of the real-space cell list: cells at least rcut/kRealSub wide along
 // every fractional axis (perpendicular widths of the box from iL).  False when
 // rcut exceeds half the smallest width (the minimum image would not be unique).
 static bool real_grid(const Handle *h, double rcut, int nb[3]) {
@@ -677,9 +677,9 @@ static bool real_grid(const Handle *h, double rcut, int nb[3]) {
                         1.0 / sqrt(c.iL11 * c.iL11 + c.iL21 * c.iL21), 1.0 / fabs(c.iL22)};
   const double wmin = fmin(wd[0], fmin(wd[1], wd[2]));
   if (!(rcut > 0.0) || rcut > 0.5 * wmin) return false;
-  for (int d = 0; d < 3; d++) {
-    const double m = floor(wd[d] / rcut);
-    nb[d] = m < 1.0 ? 1 : (m > 512.0 ? 512 : (int)m);
+  for (int d = 0; d < 3; d++) {  // cells at least rcut / kRealSub wide
+    const double m = floor(kRealSub * wd[d] / rcut);
+    nb[d] = m < 1.0 ? 1 : (m > 1023.0 ? 1023 : (int)m);
   }
   return true;
 }

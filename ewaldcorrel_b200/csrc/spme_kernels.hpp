@@ -146,6 +146,9 @@ int launch_sk_radial(const Geom &g, const double *acc, int nbins, double dk, dou
                      double *counts, cudaStream_t st);
 
 // ---- real-space term (k_real.cu) ----
+// Coarse cells of the real-space cell list are at least rcut / kRealSub wide;
+// the pair kernel searches kRealSub cells either side.
+constexpr int kRealSub = 2;
 // Cell sort of the points on the coarse grid `coarse` (cells >= rcut wide),
 // then the minimum-image erfc pair sum: dx (n x 3, input order, may be null)
 // and out (device, 10 doubles: E_real, E_self, E_net, virial[6], net-charge
