@@ -126,3 +126,47 @@ int launch_sk_radial(const Geom &g, const double *acc, int nbins, double dk, dou
 }
 
 }  // namespace spme
+
+namespace spme {
+
+// ---------------------------------------------------------------------------
+// Cross-correlations of several densities (gmx_ewald.py:76-95): after each
+// density's sfac, its structure factor is kept in slot i (FP32 complex);
+// once all D slots of a frame are filled, C_k += Q_i conj(Q_j) for every
+// pair i <= j (k in row order: (0,0), (0,1), ..., (1,1), ...), FP64 complex,
+// one writer per (pair, mode).
+__global__ void __launch_bounds__(256) xc_store_kernel(long nmodes, const float2 *__restrict__ S,
+                                                       float2 *__restrict__ slot) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nmodes; i += (long)gridDim.x * blockDim.x)
+    slot[i] = S[i];
+}
+
+__global__ void __launch_bounds__(256) xc_accumulate_kernel(long nmodes, int D, const float2 *__restrict__ Q,
+                                                            double2 *__restrict__ C) {
+  for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < nmodes; m += (long)gridDim.x * blockDim.x) {
+    int k = 0;
+    for (int i = 0; i < D; i++) {
+      const float2 a = Q[(long)i * nmodes + m];
+      for (int j = i; j < D; j++, k++) {
+        const float2 b = Q[(long)j * nmodes + m];
+        double2 c = C[(long)k * nmodes + m];
+        // a * conj(b)
+        c.x += (double)a.x * b.x + (double)a.y * b.y;
+        c.y += (double)a.y * b.x - (double)a.x * b.y;
+        C[(long)k * nmodes + m] = c;
+      }
+    }
+  }
+}
+
+int launch_xc_store(long nmodes, const float2 *S, float2 *slot, cudaStream_t st) {
+  xc_store_kernel<<<4 * 148, 256, 0, st>>>(nmodes, S, slot);
+  return 1;
+}
+
+int launch_xc_accumulate(long nmodes, int D, const float2 *Q, double2 *C, cudaStream_t st) {
+  xc_accumulate_kernel<<<4 * 148, 256, 0, st>>>(nmodes, D, Q, C);
+  return 1;
+}
+
+}  // namespace spme

@@ -57,6 +57,11 @@ struct Handle {
   long long sk_frames = 0;
   double *d_skpart = nullptr, *d_skres = nullptr;
   int sk_cap = 0;
+  // cross-correlations of several densities: D stored S, D(D+1)/2 sums
+  int xc_D = 0;
+  long long xc_frames = 0;
+  float2 *d_xcq = nullptr;
+  double2 *d_xcc = nullptr;
   // real-space term: coarse cell sort and per-point records
   struct RealBufs {
     SortBuffers sb{};
@@ -313,6 +318,8 @@ void destroy(Handle *h) {
   dfree(h->d_sk);
   dfree(h->d_skpart);
   dfree(h->d_skres);
+  dfree(h->d_xcq);
+  dfree(h->d_xcc);
   if (h->s_in) cudaStreamDestroy(h->s_in);
   if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -787,6 +794,54 @@ int sfac_sk_radial(void *p, int nbins, double kmax, double *sums, double *counts
   if (!launched(h, k, "sk radial")) return 2;
   if (!CK(h, cudaMemcpyAsync(sums, h->d_skres, sizeof(double) * nbins, cudaMemcpyDeviceToHost, h->stream)) ||
       !CK(h, cudaMemcpyAsync(counts, h->d_skres + nbins, sizeof(double) * nbins, cudaMemcpyDeviceToHost, h->stream)))
+    return 2;
+  return sync(h) ? 0 : 2;
+}
+
+int sfac_xc_reset(void *p, int D) {
+  Handle *h = H(p);
+  if (!h || D < 1 || D > 64) return 1;
+  const size_t nm = (size_t)h->nmodes, npair = (size_t)D * (D + 1) / 2;
+  if (D != h->xc_D) {
+    dfree(h->d_xcq);
+    dfree(h->d_xcc);
+    h->xc_D = 0;
+    if (!dalloc(h, &h->d_xcq, (size_t)D * nm) || !dalloc(h, &h->d_xcc, npair * nm)) return 2;
+    h->xc_D = D;
+  }
+  h->xc_frames = 0;
+  return CK(h, cudaMemsetAsync(h->d_xcc, 0, sizeof(double2) * npair * nm, h->stream)) &&
+                 CK(h, cudaMemsetAsync(h->d_xcq, 0, sizeof(float2) * (size_t)D * nm, h->stream))
+             ? 0
+             : 2;
+}
+
+int sfac_xc_store(void *p, int i) {
+  Handle *h = H(p);
+  if (!h || i < 0 || i >= h->xc_D) return 1;
+  if (h->state != 0) {
+    printf("Error: You must call sfac before this routine.\n");
+    return 1;
+  }
+  const int k = launch_xc_store(h->nmodes, h->d_cplx, h->d_xcq + (size_t)i * h->nmodes, h->stream);
+  return launched(h, k, "xc store") ? 0 : 2;
+}
+
+int sfac_xc_accumulate(void *p) {
+  Handle *h = H(p);
+  if (!h || h->xc_D < 1) return 1;
+  const int k = launch_xc_accumulate(h->nmodes, h->xc_D, h->d_xcq, h->d_xcc, h->stream);
+  if (!launched(h, k, "xc accumulate")) return 2;
+  h->xc_frames++;
+  return 0;
+}
+
+int sfac_xc_get(void *p, int k, double *out, long long *frames) {
+  Handle *h = H(p);
+  if (!h || !out || h->xc_D < 1 || k < 0 || k >= h->xc_D * (h->xc_D + 1) / 2) return 1;
+  if (frames) *frames = h->xc_frames;
+  if (!CK(h, cudaMemcpyAsync(out, h->d_xcc + (size_t)k * h->nmodes, sizeof(double2) * h->nmodes,
+                             cudaMemcpyDeviceToHost, h->stream)))
     return 2;
   return sync(h) ? 0 : 2;
 }

@@ -145,6 +145,10 @@ size_t sk_partial_words();
 int launch_sk_radial(const Geom &g, const double *acc, int nbins, double dk, double *partials, double *sums,
                      double *counts, cudaStream_t st);
 
+// cross-correlations of D densities: slot i <- S; C_k += Q_i conj(Q_j), i <= j
+int launch_xc_store(long nmodes, const float2 *S, float2 *slot, cudaStream_t st);
+int launch_xc_accumulate(long nmodes, int D, const float2 *Q, double2 *C, cudaStream_t st);
+
 // ---- real-space term (k_real.cu) ----
 // Coarse cells of the real-space cell list are at least rcut / kRealSub wide;
 // the pair kernel searches kRealSub cells either side.

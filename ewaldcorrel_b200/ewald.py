@@ -77,6 +77,10 @@ def describe_sfac():
     decl(lib.sfac_sk_accumulate, c_int, sfac_p)
     decl(lib.sfac_sk_get, c_int, sfac_p, nparr, POINTER(c_longlong))
     decl(lib.sfac_sk_radial, c_int, sfac_p, c_int, c_double, nparr, nparr)
+    decl(lib.sfac_xc_reset, c_int, sfac_p, c_int)
+    decl(lib.sfac_xc_store, c_int, sfac_p, c_int)
+    decl(lib.sfac_xc_accumulate, c_int, sfac_p)
+    decl(lib.sfac_xc_get, c_int, sfac_p, c_int, nparr, POINTER(c_longlong))
     intarr = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     decl(lib.sfac_debug_sort, c_int, sfac_p, c_int, intarr, intarr)
     decl(lib.sfac_debug_spread, c_int, sfac_p,
@@ -205,6 +209,34 @@ class Sfac:
         if self._libsfac.sfac_sk_radial(self._data, int(nbins), float(kmax), sums, counts) != 0:
             raise RuntimeError("sfac_sk_radial failed")
         return sums, counts
+
+    # cross-correlations of several densities (additions; gmx_ewald.py:76-95)
+    def xc_reset(self, D):
+        if self._libsfac.sfac_xc_reset(self._data, int(D)) != 0:
+            raise RuntimeError("sfac_xc_reset failed")
+        self._xc_D = int(D)
+
+    def xc_store(self, i):
+        """Keeps the structure factor of the last sfac() as density i."""
+        if self._libsfac.sfac_xc_store(self._data, int(i)) != 0:
+            raise RuntimeError("sfac_xc_store failed (call xc_reset, then sfac)")
+
+    def xc_accumulate(self):
+        """C[k] += Q[i] conj(Q[j]) for i <= j over the stored densities."""
+        if self._libsfac.sfac_xc_accumulate(self._data) != 0:
+            raise RuntimeError("sfac_xc_accumulate failed")
+
+    def xc_get(self):
+        """(C as a (D(D+1)/2, K0, K1, ldim) complex array, number of frames)."""
+        D = self._xc_D
+        C = np.zeros((D * (D + 1) // 2, self.K[0], self.K[1], self.ldim), np.complex128)
+        frames = c_longlong(0)
+        for k in range(C.shape[0]):
+            buf = np.zeros(2 * C[k].size)
+            if self._libsfac.sfac_xc_get(self._data, k, buf, byref(frames)) != 0:
+                raise RuntimeError("sfac_xc_get failed")
+            C[k] = (buf[0::2] + 1j * buf[1::2]).reshape(C[k].shape)
+        return C, int(frames.value)
 
     # diagnostics (additions)
     def last_error(self):

@@ -102,6 +102,21 @@ int sfac_sk_accumulate(void *sfac);
 int sfac_sk_get(void *sfac, double *out, long long *frames);
 int sfac_sk_radial(void *sfac, int nbins, double kmax, double *sums, double *counts);
 
+/* Cross-correlations of D densities, on the device: what the reference's
+ * gmx_ewald.py:76-95 does on the host (Q[i] = S after each density's sfac;
+ * C[k] += Q[i] conj(Q[j]) for i <= j, k counting the pairs in row order).
+ * No counterpart in the reference's library.
+ *   sfac_xc_reset       D slots (1..64), zeroes the sums and the frame count;
+ *   sfac_xc_store       after sfac: keeps this density's S in slot i;
+ *   sfac_xc_accumulate  adds Q[i] conj(Q[j]) of the stored slots (FP64);
+ *   sfac_xc_get         copies sum k (K0 x K1 x ldim complex as interleaved
+ *                       doubles, get_S's mode order) and the frame count.
+ * Return 0, 1 on bad arguments or state, 2 on a CUDA error. */
+int sfac_xc_reset(void *sfac, int D);
+int sfac_xc_store(void *sfac, int i);
+int sfac_xc_accumulate(void *sfac);
+int sfac_xc_get(void *sfac, int k, double *out, long long *frames);
+
 /* Real-space Ewald term and corrections beside the reciprocal sum: with the
  * Ewald influence function of splitting parameter eta (sfac_set_ewald, or
  * ewald.py's ewald_f), E_recip + out[0] + out[1] + out[2] is the full Ewald

@@ -1,6 +1,7 @@
-"""Structure-factor analysis on the device (sfac_sk_*): the sum of |S|^2 over
-frames (run.py:27-47) and its radial binning (plot.py:9-32) against the FP64
-oracle."""
+"""Structure-factor analysis on the device against the FP64 oracle: the sum
+of |S|^2 over frames (sfac_sk_*, run.py:27-47), its radial binning
+(plot.py:9-32), and the cross-correlations of several densities (sfac_xc_*,
+gmx_ewald.py:76-95)."""
 import numpy as np
 import pytest
 
@@ -63,3 +64,36 @@ def test_sk_needs_sfac_first():
     g = E().Sfac(np.array([3.0, 3.0, 3.0, 0, 0, 0]), np.array([16, 16, 16]), 4)
     with pytest.raises(RuntimeError):
         g.sk_accumulate()
+
+
+def test_cross_correlations_match_oracle():
+    """gmx_ewald.py:76-95: per frame, S of each of D densities (own points and
+    weights), then C[k] += Q[i] conj(Q[j]) for i <= j."""
+    rng = np.random.default_rng(12)
+    L = np.array([4.2, 4.0, 4.4, 0.5, -0.3, 0.2])
+    K = (32, 30, 36)
+    D = 3
+    g = E().Sfac(L, np.array(K), 4)
+    o = O.OracleSfac(L, np.array(K), 4)
+    g.xc_reset(D)
+    npair = D * (D + 1) // 2
+    ref = np.zeros((npair,) + g.get_S().shape, np.complex128)
+    for _ in range(2):
+        Q = []
+        for i in range(D):
+            n = 300 + 100 * i
+            x = rng.uniform(-2, 6, size=(n, 3))
+            w = rng.normal(size=n)
+            g.sfac(w, x)
+            g.xc_store(i)
+            o.sfac(w, x)
+            Q.append(np.array(o.get_S()))
+        g.xc_accumulate()
+        k = 0
+        for i in range(D):
+            for j in range(i, D):
+                ref[k] += Q[i] * np.conj(Q[j])
+                k += 1
+    C, nf = g.xc_get()
+    assert nf == 2
+    assert np.abs(C - ref).max() <= 2e-5 * np.abs(ref).max()
