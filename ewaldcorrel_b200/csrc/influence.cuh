@@ -28,10 +28,11 @@ __device__ __forceinline__ double ewald_f(double r2, double fac, double &fp) {
 // (sfac.cpp:240-289, same sphere bounds, FP64 without contraction).  The
 // conjugate images that set_A folds onto interior modes have the same f
 // values, so the caller doubles those instead of revisiting them.
-__device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1, int K2, int kx, int ky, int kz,
-                             double &sf, double sd[6]) {
+// F: f(m^2) returning f and storing f'(m^2) in fp.
+template <class F>
+__device__ __forceinline__ void radial_images(const InfConst &inf, const F &fn, int K0, int K1, int K2, int kx, int ky,
+                                              int kz, double &sf, double sd[6]) {
   const double R2 = __dmul_rn(inf.max_m, inf.max_m);
-  const double fac = inf.fac;
   const int i0 = __double2int_rz(__ddiv_rn(inf.max_m, inf.iL00));
   sf = 0.0;
   for (int c = 0; c < 6; c++) sd[c] = 0.0;
@@ -53,7 +54,7 @@ __device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1
         const double mz = __dadd_rn(mz0, __dmul_rn((double)k, inf.iL22));
         const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
         double fp;
-        sf += ewald_f(m2, fac, fp);
+        sf += fn(m2, fp);
         sd[0] += fp * mx * mx;
         sd[1] += fp * my * my;
         sd[2] += fp * mz * mz;
@@ -63,6 +64,42 @@ __device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1
       }
     }
   }
+}
+
+struct EwaldRadial {
+  double fac;
+  __device__ __forceinline__ double operator()(double m2, double &fp) const { return ewald_f(m2, fac, fp); }
+};
+
+// A radial function sampled by the caller: f and f' at m^2 = k dm2,
+// k = 0..nt-1, evaluated by cubic Hermite interpolation in m^2 (f to fourth
+// order in dm2, f' as the interpolant's derivative to third order); 0 beyond
+// the last sample.
+struct TableRadial {
+  const double *f, *df;
+  int nt;
+  double dm2, inv_dm2;
+  __device__ __forceinline__ double operator()(double m2, double &fp) const {
+    const double t = m2 * inv_dm2;
+    if (!(t <= (double)(nt - 1))) {
+      fp = 0.0;
+      return 0.0;
+    }
+    int k = (int)t;
+    if (k > nt - 2) k = nt - 2;
+    const double u = t - (double)k, u2 = u * u, u3 = u2 * u;
+    const double p0 = f[k], p1 = f[k + 1], m0 = df[k] * dm2, m1 = df[k + 1] * dm2;
+    const double v = (2.0 * u3 - 3.0 * u2 + 1.0) * p0 + (u3 - 2.0 * u2 + u) * m0 + (3.0 * u2 - 2.0 * u3) * p1 +
+                     (u3 - u2) * m1;
+    fp = ((6.0 * u2 - 6.0 * u) * p0 + (3.0 * u2 - 4.0 * u + 1.0) * m0 + (6.0 * u - 6.0 * u2) * p1 +
+          (3.0 * u2 - 2.0 * u) * m1) * inv_dm2;
+    return v;
+  }
+};
+
+__device__ __forceinline__ void ewald_images(const InfConst &inf, int K0, int K1, int K2, int kx, int ky, int kz,
+                                             double &sf, double sd[6]) {
+  radial_images(inf, EwaldRadial{inf.fac}, K0, K1, K2, kx, ky, kz, sf, sd);
 }
 
 

@@ -121,6 +121,35 @@ int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *d
   return 1;
 }
 
+// Tabulates a caller-sampled radial function (TableRadial) per stored mode,
+// over the same image set as set_A (radial_images), into set_A's table
+// layout: A = (1/2 on the kz = 0 / Nyquist planes) sum f, dA = 2 x that
+// weight x sum f' m m.
+__global__ void __launch_bounds__(256) radial_table_kernel(Geom g, InfConst ic, TableRadial fn, double *__restrict__ A,
+                                                           double *__restrict__ dA) {
+  const long nmodes = (long)g.K0 * g.K1 * g.ldim;
+  const bool even = (g.K2 % 2) == 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nmodes; i += (long)gridDim.x * blockDim.x) {
+    const int kz = (int)(i % g.ldim);
+    const long r = i / g.ldim;
+    const int ky = (int)(r % g.K1), kx = (int)(r / g.K1);
+    const bool plane = (kz == 0) || (even && kz == g.ldim - 1);
+    double sf, sd[6];
+    radial_images(ic, fn, g.K0, g.K1, g.K2, kx, ky, kz, sf, sd);
+    const double wA = plane ? 0.5 : 1.0;
+    A[i] = wA * sf;
+#pragma unroll
+    for (int c = 0; c < 6; c++) dA[6 * i + c] = 2.0 * wA * sd[c];
+  }
+}
+
+int launch_radial_table(const Geom &g, const InfConst &ic, const double *f, const double *df, int nt, double dm2,
+                        double *A, double *dA, cudaStream_t st) {
+  TableRadial fn{f, df, nt, dm2, 1.0 / dm2};
+  radial_table_kernel<<<4 * 148, 256, 0, st>>>(g, ic, fn, A, dA);
+  return 1;
+}
+
 int launch_finish(const double *partials, int nblocks, const CellConst *cell, double *raw, double *ev,
                   cudaStream_t st) {
   conv_finish_kernel<<<1, 8 * 32, 0, st>>>(partials, nblocks, cell, raw, ev);

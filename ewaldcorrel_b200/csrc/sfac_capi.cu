@@ -29,7 +29,7 @@ struct Handle {
   Spline spline{};
   SplineNodes nodes{};
   int state = -1;  // -1: nothing computed, 0: structure factor, 1: potential grid
-  int a_mode = 0;  // 0: no influence function, 1: host tables, 2: Ewald on device
+  int a_mode = 0;  // 0: no influence function, 1: host tables, 2: Ewald on device, 3: sampled radial function
   Influence inf{};
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is enqueued on
@@ -844,6 +844,39 @@ int sfac_xc_get(void *p, int k, double *out, long long *frames) {
                              cudaMemcpyDeviceToHost, h->stream)))
     return 2;
   return sync(h) ? 0 : 2;
+}
+
+int sfac_set_radial(void *p, int nt, const double *f, const double *df, double m2max, double max_m) {
+  Handle *h = H(p);
+  if (!h) return 1;
+  if (nt < 2 || !f || !df || !(m2max > 0.0) || !(max_m >= 0.0) || max_m * max_m > m2max) {
+    printf("sfac_set_radial: need nt >= 2 samples on [0, m2max] with max_m^2 <= m2max\n");
+    return 1;
+  }
+  const size_t nm = (size_t)h->nmodes;
+  double *dtab = nullptr;
+  if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
+  if (!dalloc(h, &dtab, 2 * (size_t)nt)) return 2;
+  const CellConst &c = h->hcell;
+  const InfConst ic{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, 0.0, max_m, 0.0};
+  bool ok = CK(h, cudaMemcpyAsync(dtab, f, sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream)) &&
+            CK(h, cudaMemcpyAsync(dtab + nt, df, sizeof(double) * nt, cudaMemcpyHostToDevice, h->stream));
+  if (ok) {
+    const int k = launch_radial_table(h->geom, ic, dtab, dtab + nt, nt, m2max / (nt - 1), h->d_A, h->d_A + nm,
+                                      h->stream);
+    ok = launched(h, k, "radial table") && sync(h);
+  }
+  dfree(dtab);
+  if (!ok) return 3;
+  Influence inf{};
+  inf.mode = 1;
+  inf.A = h->d_A;
+  inf.dA = h->d_A + nm;
+  inf.K2d = FastDiv((uint32_t)h->K[2]);
+  if (h->a_mode != 3 || memcmp(&inf, &h->inf, sizeof(Influence)) != 0) h->version++;
+  h->inf = inf;
+  h->a_mode = 3;
+  return 0;
 }
 
 int sfac_set_ewald(void *p, double beta, double max_m) {

@@ -114,6 +114,10 @@ int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStr
 // Tabulates a mode-2 influence function as FP64 tables A (nmodes) and dA
 // (6 per mode), the layout of mode 1.
 int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *dA, cudaStream_t st);
+// Tables A / dA (mode 1 layout) of a caller-sampled radial function f, f'
+// at m^2 = k dm2 (k < nt), over set_A's image set within ic.max_m.
+int launch_radial_table(const Geom &g, const InfConst &ic, const double *f, const double *df, int nt, double dm2,
+                        double *A, double *dA, cudaStream_t st);
 constexpr int kConvBlocks = 592;  // 4 x 148 SMs: fixed, so the reduction order is fixed
 constexpr int kRedWords = 8;      // e, v00, v11, v22, v10, v20, v21, pad
 // Energy/virial sums over S without modifying it (en): raw sums -> out,

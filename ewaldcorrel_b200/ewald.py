@@ -68,6 +68,7 @@ def describe_sfac():
     decl(lib.potl, None, sfac_p, c_int, nparr, nparr)
     # additions
     decl(lib.sfac_set_ewald, c_int, sfac_p, c_double, c_double)
+    decl(lib.sfac_set_radial, c_int, sfac_p, c_int, nparr, nparr, c_double, c_double)
     decl(lib.sfac_last_error, c_int, sfac_p)
     decl(lib.sfac_error_string, c_char_p, sfac_p)
     decl(lib.sfac_device, c_int, sfac_p)
@@ -153,6 +154,22 @@ class Sfac:
         if n != 0:
             raise RuntimeError("Error (%d) setting the Ewald kernel." % n)
 
+    def set_radial(self, f, df, max_m, m2max=None, samples=200001):
+        """A radial influence function evaluated on the device (an addition:
+        set_A calls a host function once per lattice vector).  f, df:
+        vectorised callables giving f(m^2) and f'(m^2), sampled at `samples`
+        points of [0, m2max] (default max_m^2)."""
+        m2max = float(max_m) ** 2 if m2max is None else float(m2max)
+        z = np.linspace(0.0, m2max, int(samples))
+        fv = np.ascontiguousarray(f(z), dtype=np.float64)
+        dv = np.ascontiguousarray(df(z), dtype=np.float64)
+        self.__dict__.pop("f", None)
+        self.__dict__.pop("_ewald", None)
+        self._radial = (f, df, float(max_m), m2max, int(samples))
+        n = self._libsfac.sfac_set_radial(self._data, len(z), fv, dv, m2max, float(max_m))
+        if n != 0:
+            raise RuntimeError("Error (%d) setting the radial kernel." % n)
+
     def set_L(self, L):
         """Replaces the box.  Like the reference wrapper (ewald.py:119-122),
         a host influence function is re-tabulated with max_m = 1.0; an
@@ -162,6 +179,9 @@ class Sfac:
             self.set_A(self.f, 1.0)
         elif hasattr(self, "_ewald"):
             self.set_ewald(*self._ewald)
+        elif hasattr(self, "_radial"):
+            f, df, max_m, m2max, samples = self._radial
+            self.set_radial(f, df, max_m, m2max, samples)
 
     def real_space(self, w, x, eta, rcut, grad=True):
         """Real-space Ewald term beside this solver's reciprocal sum (an

@@ -138,6 +138,15 @@ int sfac_real_space(void *sfac, int n, const double *w, const double *x, double 
 int sfac_real_space_device(void *sfac, int n, const double *x, const double *w, double eta, double rcut, double *out,
                            double *dx);
 
+/* Any radial influence function on the device, in place of set_A's host
+ * callback (sfac.hpp:201-203): f(m^2) and f'(m^2) sampled by the caller at
+ * m^2 = k m2max/(nt-1), k = 0..nt-1, are interpolated (cubic Hermite in m^2,
+ * FP64) over the same images set_A visits (|m| < max_m, max_m^2 <= m2max) and
+ * tabulated as set_A's A and dA.  Like set_A, later box changes do not
+ * re-tabulate.  Returns 0, 1 on bad arguments, 2 or 3 on a CUDA error.
+ * No counterpart in the reference (set_A evaluates f on the host). */
+int sfac_set_radial(void *sfac, int nt, const double *f, const double *df, double m2max, double max_m);
+
 /* Last CUDA or argument error seen by this handle (0 = none), and its text. */
 int sfac_last_error(void *sfac);
 const char *sfac_error_string(void *sfac);
