@@ -170,7 +170,7 @@ __device__ __forceinline__ void ewald_images_row(const InfConst &inf, const Fast
 // The device Ewald constants, or zeros when the influence comes from tables.
 __device__ __forceinline__ InfConst load_ic(const Influence &inf) {
   InfConst c{};
-  if (inf.mode == 2) c = *inf.ic;
+  if (inf.mode >= 2) c = *inf.ic;
   return c;
 }
 
@@ -245,6 +245,59 @@ __device__ __forceinline__ double mode_influence_acc(const Influence &inf, const
   const double A = wA * sf;
   acc[0] += sq * A;
   return A;
+}
+
+// Mode 4, one stored mode: A from the compact table; for a single image the
+// lattice vector (kx + si K0, ky + sj K1, kz + sk K2) gives m and
+// dA = 2 wA f'(m^2) m m = 2 (fac - 1/m^2) A m m (A = wA f); several images
+// take mode 2's row enumeration (multi).  Adds sq A and sq dA to acc.
+__device__ __forceinline__ double ewald_row_acc_multi(const Influence &inf, const InfConst &ic, const Geom &g, long i,
+                                                   int kx, int ky, int kz, bool plane, double sq, double *acc) {
+  double a7[7] = {0, 0, 0, 0, 0, 0, 0};
+  Influence m2 = inf;
+  m2.mode = 2;
+  const double A = mode_influence_acc(m2, ic, g, i, kx, ky, kz, plane, sq, a7);
+#pragma unroll
+  for (int c = 0; c < 7; c++) acc[c] += a7[c];
+  return A;
+}
+
+__device__ __forceinline__ double compact_acc(const Influence &inf, const InfConst &ic, const Geom &g, long i, int kx,
+                                              int ky, int kz, bool plane, double sq, double A, uint8_t code,
+                                              double (&acc)[7]) {
+  if (code == kImgMany) return ewald_row_acc_multi(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
+  if (code == kImgNone || A == 0.0) return 0.0;
+  const double ii = (double)(kx + ((int)(code & 3) - 2) * g.K0);
+  const double jj = (double)(ky + ((int)((code >> 2) & 3) - 2) * g.K1);
+  const double kk = (double)(kz + ((int)((code >> 4) & 3) - 2) * g.K2);
+  const double mx = ii * ic.iL00;
+  const double my = ii * ic.iL10 + jj * ic.iL11;
+  const double mz = ii * ic.iL20 + jj * ic.iL21 + kk * ic.iL22;
+  const double m2 = mx * mx + my * my + mz * mz;
+  const double t = 2.0 * (ic.fac - __drcp_rn(m2)) * A * sq;
+  acc[0] += sq * A;
+  acc[1] += t * mx * mx;
+  acc[2] += t * my * my;
+  acc[3] += t * mz * mz;
+  acc[4] += t * my * mx;
+  acc[5] += t * mz * mx;
+  acc[6] += t * mz * my;
+  return A;
+}
+
+// The influence source fixed at compile time (one kernel per source keeps
+// each variant's registers to its own path): IM = 1 tables, 2 row tables
+// (mode 2), 4 compact table (mode 4).
+template <int IM>
+__device__ __forceinline__ double influence_acc(const Influence &inf, const InfConst &ic, const Geom &g, long i, int kx,
+                                                int ky, int kz, bool plane, double sq, double (&acc)[7]) {
+  if constexpr (IM == 4) {
+    return compact_acc(inf, ic, g, i, kx, ky, kz, plane, sq, inf.A[i], inf.imgcode[i], acc);
+  } else {
+    Influence f = inf;
+    f.mode = IM;
+    return mode_influence_acc(f, ic, g, i, kx, ky, kz, plane, sq, acc);
+  }
 }
 
 __device__ __forceinline__ void block_reduce7(const double (&acc)[7], double (*red)[7], double *out_global) {

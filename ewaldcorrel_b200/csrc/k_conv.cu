@@ -121,6 +121,68 @@ int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *d
   return 1;
 }
 
+// Compact table of the device Ewald function (mode 4): A per mode and the
+// lattice shift of its image when exactly one image lies in the sphere.
+__global__ void __launch_bounds__(256) ewald_compact_kernel(Geom g, Influence inf, double *__restrict__ A,
+                                                            uint8_t *__restrict__ code) {
+  const long nmodes = (long)g.K0 * g.K1 * g.ldim;
+  const InfConst ic = *inf.ic;
+  const bool even = (g.K2 % 2) == 0;
+  const int K0 = g.K0, K1 = g.K1, K2 = g.K2;
+  for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < nmodes; m += (long)gridDim.x * blockDim.x) {
+    const int kz = (int)(m % g.ldim);
+    const long r = m / g.ldim;
+    const int ky = (int)(r % K1), kx = (int)(r / K1);
+    const bool plane = (kz == 0) || (even && kz == g.ldim - 1);
+    // set_A's image set (radial_images' loops), counting the images
+    const double R2 = __dmul_rn(ic.max_m, ic.max_m);
+    const int i0 = __double2int_rz(__ddiv_rn(ic.max_m, ic.iL00));
+    double sf = 0.0;
+    int count = 0, li = 0, lj = 0, lk = 0;
+    for (int i = -i0 + imod(kx + i0, K0); i <= i0; i += K0) {
+      const double mx = __dmul_rn((double)i, ic.iL00);
+      const double m20 = __dmul_rn(mx, mx);
+      const double dy = sqrt(fmax(__dsub_rn(R2, m20), 0.0));
+      const double my0 = __dmul_rn((double)i, ic.iL10);
+      const int j0 = (int)ceil(__ddiv_rn(__dsub_rn(-dy, my0), ic.iL11));
+      const int j1 = (int)floor(__ddiv_rn(__dsub_rn(dy, my0), ic.iL11));
+      for (int j = j0 + imod(ky - j0, K1); j <= j1; j += K1) {
+        const double my = __dadd_rn(my0, __dmul_rn((double)j, ic.iL11));
+        const double m21 = __dadd_rn(m20, __dmul_rn(my, my));
+        const double dz = sqrt(fmax(__dsub_rn(R2, m21), 0.0));
+        const double mz0 = __dadd_rn(__dmul_rn((double)i, ic.iL20), __dmul_rn((double)j, ic.iL21));
+        const int k0 = (int)ceil(__ddiv_rn(__dsub_rn(-dz, mz0), ic.iL22));
+        const int k1 = (int)floor(__ddiv_rn(__dsub_rn(dz, mz0), ic.iL22));
+        for (int k = k0 + imod(kz - k0, K2); k <= k1; k += K2) {
+          const double mz = __dadd_rn(mz0, __dmul_rn((double)k, ic.iL22));
+          const double m2 = __dadd_rn(m21, __dmul_rn(mz, mz));
+          double fp;
+          sf += ewald_f(m2, ic.fac, fp);
+          count++;
+          li = i;
+          lj = j;
+          lk = k;
+        }
+      }
+    }
+    A[m] = (plane ? 0.5 : 1.0) * sf;
+    uint8_t c = kImgMany;
+    if (count == 0) {
+      c = kImgNone;
+    } else if (count == 1) {
+      const int si = (li - kx) / K0, sj = (lj - ky) / K1, sk = (lk - kz) / K2;
+      if (si >= -2 && si <= 1 && sj >= -2 && sj <= 1 && sk >= -2 && sk <= 1)
+        c = (uint8_t)((si + 2) | ((sj + 2) << 2) | ((sk + 2) << 4));
+    }
+    code[m] = c;
+  }
+}
+
+int launch_ewald_compact(const Geom &g, const Influence &inf, double *A, uint8_t *imgcode, cudaStream_t st) {
+  ewald_compact_kernel<<<4 * 148, 256, 0, st>>>(g, inf, A, imgcode);
+  return 1;
+}
+
 // Tabulates a caller-sampled radial function (TableRadial) per stored mode,
 // over the same image set as set_A (radial_images), into set_A's table
 // layout: A = (1/2 on the kz = 0 / Nyquist planes) sum f, dA = 2 x that

@@ -10,6 +10,8 @@
 // 7 butterflies written out and a direct-DFT butterfly for any other prime,
 // and stores the lines back.  Twiddles come from an FP32 table built in FP64
 // (fft_twiddle_kernel).
+#include <type_traits>
+
 #include "fft_engine.cuh"
 #include "fft_reg.cuh"
 #include "influence.cuh"
@@ -367,7 +369,7 @@ __global__ void __launch_bounds__(256) fft_x_kernel(FftLen L, Geom g, Influence 
 // The reciprocal step happens on the step-2 registers (all kx = k1 + n1*k2
 // of the line), so forward transform, convolution and inverse transform cost
 // two exchanges in total.
-template <int MODE>
+template <int MODE, int IM>
 __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, const float2 *__restrict__ twg, Geom g,
                                                      Influence inf, const double *__restrict__ iB0,
                                                      const double *__restrict__ iB1, const double *__restrict__ iB2,
@@ -426,7 +428,7 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
             data[line + (long)kx * nlines] = cscale(w[k2], (float)(iB0[kx] * s12));
           }
         }
-      } else if (inf.mode == 1) {
+      } else if (IM == 1) {
         // tabulated influence function: the line's values stay in registers
         // and all R modes' table loads are in flight together
         if (live) {
@@ -480,7 +482,7 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
             const double ib = iB0[kx] * s12;
             double sq = (double)q.x * q.x + (double)q.y * q.y;
             if (MODE == XM_FWD_CONV_INV) sq *= ib * ib;  // |F iB|^2
-            const double A = mode_influence_acc(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
+            const double A = influence_acc<IM>(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
             if (MODE != XM_EN) {
               double f = A * ib * (MODE == XM_FWD_CONV_INV ? ib : 1.0);
               if (plane) f *= 2.0;
@@ -766,11 +768,12 @@ void fft_prepare_kernels() {
   cudaFuncSetAttribute((const void *)fft_x_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        lim);
   cudaFuncSetAttribute((const void *)fft_x_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_FWD_DECONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_FWD_CONV_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       lim);
-  cudaFuncSetAttribute((const void *)fft_x2_kernel<XM_EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  const void *x2[] = {(const void *)fft_x2_kernel<XM_FWD_DECONV, 1>, (const void *)fft_x2_kernel<XM_CONV_INV, 1>,
+                      (const void *)fft_x2_kernel<XM_CONV_INV, 2>, (const void *)fft_x2_kernel<XM_CONV_INV, 4>,
+                      (const void *)fft_x2_kernel<XM_FWD_CONV_INV, 1>, (const void *)fft_x2_kernel<XM_FWD_CONV_INV, 2>,
+                      (const void *)fft_x2_kernel<XM_FWD_CONV_INV, 4>, (const void *)fft_x2_kernel<XM_EN, 1>,
+                      (const void *)fft_x2_kernel<XM_EN, 2>, (const void *)fft_x2_kernel<XM_EN, 4>};
+  for (const void *f : x2) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute((const void *)fft_y2_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute((const void *)fft_y2_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute((const void *)fft_zr2c2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -963,8 +966,14 @@ static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const 
     const int B = 1 << lgB;
     const size_t smem = (size_t)(n + (size_t)B * n) * sizeof(float2);
     nblocks = (int)((nl + B - 1) / B);
-    fft_x2_kernel<MODE><<<nblocks, threads, smem, st>>>(n, n1, n2, F.len[0].tw, g, inf, iB0, iB1, iB2, cplx, lgB,
-                                                        partials);
+    auto go = [&](auto IMC) {
+      constexpr int IM = decltype(IMC)::value;
+      fft_x2_kernel<MODE, IM><<<nblocks, threads, smem, st>>>(n, n1, n2, F.len[0].tw, g, inf, iB0, iB1, iB2, cplx,
+                                                              lgB, partials);
+    };
+    if (MODE == XM_FWD_DECONV || inf.mode == 1) go(std::integral_constant<int, 1>{});
+    else if (inf.mode == 4) go(std::integral_constant<int, 4>{});
+    else go(std::integral_constant<int, 2>{});
     return 1;
   }
   int B = x_lines_per_cta(F, n, nl);

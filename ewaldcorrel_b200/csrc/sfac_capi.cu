@@ -43,6 +43,7 @@ struct Handle {
   float2 *d_tw[3] = {nullptr, nullptr, nullptr};
   FftPlan3 fft{};
   double *d_A = nullptr;  // 7 * nmodes (table mode)
+  uint8_t *d_imgcode = nullptr;  // nmodes (compact Ewald table)
   RowImg *d_rows = nullptr;  // K0*K1 row image tables (device Ewald mode)
   double *d_partials = nullptr, *d_red = nullptr, *d_ev = nullptr;
   int cap = 0;
@@ -291,6 +292,7 @@ void destroy(Handle *h) {
     dfree(h->d_tw[d]);
   }
   dfree(h->d_A);
+  dfree(h->d_imgcode);
   dfree(h->d_rows);
   dfree(h->d_partials);
   dfree(h->d_ev);
@@ -905,7 +907,11 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   // keeps the per-solve evaluation.
   const size_t nm = (size_t)h->nmodes;
   bool table = 56 * nm <= kEwaldTableMaxBytes;
-  if (const char *e = getenv("SFAC_EWALD_TABLE")) table = table && !(e[0] == '0' && e[1] == 0);
+  bool compact = !table;
+  if (const char *e = getenv("SFAC_EWALD_TABLE")) {
+    if (e[0] == '0' && e[1] == 0) table = compact = false;  // evaluate the images in every solve
+    if (e[0] == 'c' && e[1] == 0) table = !(compact = true);  // compact table whatever the size
+  }
   if (table) {
     if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
     k += launch_ewald_table(h->geom, inf, h->d_A, h->d_A + nm, h->stream);
@@ -914,6 +920,15 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
     inf.A = h->d_A;
     inf.dA = h->d_A + nm;
     inf.K2d = FastDiv((uint32_t)h->K[2]);
+  } else if (compact) {
+    // A per mode and its single image's lattice shift (9 bytes per mode):
+    // dA then costs no exp in the solves
+    if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
+    if (!h->d_imgcode && !dalloc(h, &h->d_imgcode, nm)) return 2;
+    k += launch_ewald_compact(h->geom, inf, h->d_A, h->d_imgcode, h->stream);
+    inf.mode = 4;
+    inf.A = h->d_A;
+    inf.imgcode = h->d_imgcode;
   }
   if (!launched(h, k, "ewald rows")) return 3;
   if (h->a_mode != 2 || memcmp(&inf, &h->inf, sizeof(Influence)) != 0) h->version++;  // kernel arguments changed
