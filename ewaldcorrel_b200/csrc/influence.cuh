@@ -247,10 +247,11 @@ __device__ __forceinline__ double mode_influence_acc(const Influence &inf, const
   return A;
 }
 
-// Mode 4, one stored mode: A from the compact table; for a single image the
-// lattice vector (kx + si K0, ky + sj K1, kz + sk K2) gives m and
+// Mode 4, one stored mode: the packed compact-table entry; for a single image
+// the lattice vector (kx + si K0, ky + sj K1, kz + sk K2) gives m and
 // dA = 2 wA f'(m^2) m m = 2 (fac - 1/m^2) A m m (A = wA f); several images
-// take mode 2's row enumeration (multi).  Adds sq A and sq dA to acc.
+// (a negative entry) take mode 2's row enumeration.  Adds sq A and sq dA to
+// acc.
 __device__ __forceinline__ double ewald_row_acc_multi(const Influence &inf, const InfConst &ic, const Geom &g, long i,
                                                    int kx, int ky, int kz, bool plane, double sq, double *acc) {
   double a7[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -263,13 +264,16 @@ __device__ __forceinline__ double ewald_row_acc_multi(const Influence &inf, cons
 }
 
 __device__ __forceinline__ double compact_acc(const Influence &inf, const InfConst &ic, const Geom &g, long i, int kx,
-                                              int ky, int kz, bool plane, double sq, double A, uint8_t code,
+                                              int ky, int kz, bool plane, double sq, double packed,
                                               double (&acc)[7]) {
-  if (code == kImgMany) return ewald_row_acc_multi(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
-  if (code == kImgNone || A == 0.0) return 0.0;
-  const double ii = (double)(kx + ((int)(code & 3) - 2) * g.K0);
-  const double jj = (double)(ky + ((int)((code >> 2) & 3) - 2) * g.K1);
-  const double kk = (double)(kz + ((int)((code >> 4) & 3) - 2) * g.K2);
+  if (packed < 0.0) return ewald_row_acc_multi(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(packed);
+  const double A = __longlong_as_double((long long)(bits & ~0x3FULL));
+  if (A == 0.0) return 0.0;
+  const int code = (int)(bits & 0x3F);
+  const double ii = (double)(kx + ((code & 3) - 2) * g.K0);
+  const double jj = (double)(ky + (((code >> 2) & 3) - 2) * g.K1);
+  const double kk = (double)(kz + (((code >> 4) & 3) - 2) * g.K2);
   const double mx = ii * ic.iL00;
   const double my = ii * ic.iL10 + jj * ic.iL11;
   const double mz = ii * ic.iL20 + jj * ic.iL21 + kk * ic.iL22;
@@ -292,7 +296,7 @@ template <int IM>
 __device__ __forceinline__ double influence_acc(const Influence &inf, const InfConst &ic, const Geom &g, long i, int kx,
                                                 int ky, int kz, bool plane, double sq, double (&acc)[7]) {
   if constexpr (IM == 4) {
-    return compact_acc(inf, ic, g, i, kx, ky, kz, plane, sq, inf.A[i], inf.imgcode[i], acc);
+    return compact_acc(inf, ic, g, i, kx, ky, kz, plane, sq, inf.A[i], acc);
   } else {
     Influence f = inf;
     f.mode = IM;

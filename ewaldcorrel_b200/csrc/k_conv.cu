@@ -121,10 +121,11 @@ int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *d
   return 1;
 }
 
-// Compact table of the device Ewald function (mode 4): A per mode and the
-// lattice shift of its image when exactly one image lies in the sphere.
-__global__ void __launch_bounds__(256) ewald_compact_kernel(Geom g, Influence inf, double *__restrict__ A,
-                                                            uint8_t *__restrict__ code) {
+// Compact table of the device Ewald function (mode 4), one double per mode:
+// 0 when no image lies in the sphere; -1 when several do; otherwise A with
+// its 6 lowest mantissa bits replaced by the single image's lattice shift
+// (si+2) | (sj+2) << 2 | (sk+2) << 4 (a relative change below 2^-46).
+__global__ void __launch_bounds__(256) ewald_compact_kernel(Geom g, Influence inf, double *__restrict__ A) {
   const long nmodes = (long)g.K0 * g.K1 * g.ldim;
   const InfConst ic = *inf.ic;
   const bool even = (g.K2 % 2) == 0;
@@ -165,21 +166,23 @@ __global__ void __launch_bounds__(256) ewald_compact_kernel(Geom g, Influence in
         }
       }
     }
-    A[m] = (plane ? 0.5 : 1.0) * sf;
-    uint8_t c = kImgMany;
+    const double a = (plane ? 0.5 : 1.0) * sf;
+    double packed = -1.0;  // several images (or a shift out of range): row enumeration
     if (count == 0) {
-      c = kImgNone;
+      packed = 0.0;
     } else if (count == 1) {
       const int si = (li - kx) / K0, sj = (lj - ky) / K1, sk = (lk - kz) / K2;
-      if (si >= -2 && si <= 1 && sj >= -2 && sj <= 1 && sk >= -2 && sk <= 1)
-        c = (uint8_t)((si + 2) | ((sj + 2) << 2) | ((sk + 2) << 4));
+      if (si >= -2 && si <= 1 && sj >= -2 && sj <= 1 && sk >= -2 && sk <= 1) {
+        const unsigned long long c = (unsigned long long)((si + 2) | ((sj + 2) << 2) | ((sk + 2) << 4));
+        packed = __longlong_as_double((long long)((__double_as_longlong(a) & ~0x3FULL) | c));
+      }
     }
-    code[m] = c;
+    A[m] = packed;
   }
 }
 
-int launch_ewald_compact(const Geom &g, const Influence &inf, double *A, uint8_t *imgcode, cudaStream_t st) {
-  ewald_compact_kernel<<<4 * 148, 256, 0, st>>>(g, inf, A, imgcode);
+int launch_ewald_compact(const Geom &g, const Influence &inf, double *A, cudaStream_t st) {
+  ewald_compact_kernel<<<4 * 148, 256, 0, st>>>(g, inf, A);
   return 1;
 }
 

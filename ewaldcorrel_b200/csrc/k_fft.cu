@@ -387,6 +387,25 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
   const bool live = line < nlines;
   const int ky = live ? (int)(line / ldim) : 0, kz = live ? (int)(line - (long)ky * ldim) : 0;
   constexpr bool FWD = (MODE == XM_FWD_DECONV || MODE == XM_FWD_CONV_INV);
+  // compact influence table: the CTA's n x B entries are copied to shared
+  // memory (abuf[kx * B + b]) with cp.async now and used after the forward
+  // steps, so their HBM latency overlaps the transform
+  double *abuf = reinterpret_cast<double *>(ex + (size_t)B * n);
+  constexpr bool PREFETCH = (IM == 4 && MODE != XM_FWD_DECONV);
+  if (PREFETCH) {
+    for (int e = threadIdx.x; e < B * n; e += blockDim.x) {
+      const int bb = e & (B - 1), kx = e >> lgB;
+      const long ln = (long)blockIdx.x * B + bb;
+      if (ln < nlines) {
+        const int y = (int)(ln / ldim), z = (int)(ln - (long)y * ldim);
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(abuf + e);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst),
+                     "l"(inf.A + ((long)kx * K1 + y) * ldim + z)
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   __syncthreads();
   if (FWD && t < n2) {
     const int j2 = t;
@@ -401,7 +420,8 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
       for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], tw[j2 * k1]);
     });
   }
-  if (FWD) __syncthreads();
+  if (PREFETCH) asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (FWD || PREFETCH) __syncthreads();
   double acc[7];
 #pragma unroll
   for (int c = 0; c < 7; c++) acc[c] = 0.0;
@@ -482,7 +502,9 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
             const double ib = iB0[kx] * s12;
             double sq = (double)q.x * q.x + (double)q.y * q.y;
             if (MODE == XM_FWD_CONV_INV) sq *= ib * ib;  // |F iB|^2
-            const double A = influence_acc<IM>(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
+            double A;
+            if constexpr (PREFETCH) A = compact_acc(inf, ic, g, i, kx, ky, kz, plane, sq, abuf[kx * B + b], acc);
+            else A = influence_acc<IM>(inf, ic, g, i, kx, ky, kz, plane, sq, acc);
             if (MODE != XM_EN) {
               double f = A * ib * (MODE == XM_FWD_CONV_INV ? ib : 1.0);
               if (plane) f *= 2.0;
@@ -968,8 +990,9 @@ static int x_pass(const FftPlan3 &F, const Geom &g, const Influence &inf, const 
     nblocks = (int)((nl + B - 1) / B);
     auto go = [&](auto IMC) {
       constexpr int IM = decltype(IMC)::value;
-      fft_x2_kernel<MODE, IM><<<nblocks, threads, smem, st>>>(n, n1, n2, F.len[0].tw, g, inf, iB0, iB1, iB2, cplx,
-                                                              lgB, partials);
+      const size_t sm = smem + (IM == 4 && MODE != XM_FWD_DECONV ? (size_t)B * n * sizeof(double) : 0);
+      fft_x2_kernel<MODE, IM><<<nblocks, threads, sm, st>>>(n, n1, n2, F.len[0].tw, g, inf, iB0, iB1, iB2, cplx,
+                                                            lgB, partials);
     };
     if (MODE == XM_FWD_DECONV || inf.mode == 1) go(std::integral_constant<int, 1>{});
     else if (inf.mode == 4) go(std::integral_constant<int, 4>{});

@@ -43,7 +43,6 @@ struct Handle {
   float2 *d_tw[3] = {nullptr, nullptr, nullptr};
   FftPlan3 fft{};
   double *d_A = nullptr;  // 7 * nmodes (table mode)
-  uint8_t *d_imgcode = nullptr;  // nmodes (compact Ewald table)
   RowImg *d_rows = nullptr;  // K0*K1 row image tables (device Ewald mode)
   double *d_partials = nullptr, *d_red = nullptr, *d_ev = nullptr;
   int cap = 0;
@@ -292,7 +291,6 @@ void destroy(Handle *h) {
     dfree(h->d_tw[d]);
   }
   dfree(h->d_A);
-  dfree(h->d_imgcode);
   dfree(h->d_rows);
   dfree(h->d_partials);
   dfree(h->d_ev);
@@ -921,14 +919,12 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
     inf.dA = h->d_A + nm;
     inf.K2d = FastDiv((uint32_t)h->K[2]);
   } else if (compact) {
-    // A per mode and its single image's lattice shift (9 bytes per mode):
+    // A per mode with its single image's lattice shift (8 bytes per mode):
     // dA then costs no exp in the solves
     if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
-    if (!h->d_imgcode && !dalloc(h, &h->d_imgcode, nm)) return 2;
-    k += launch_ewald_compact(h->geom, inf, h->d_A, h->d_imgcode, h->stream);
+    k += launch_ewald_compact(h->geom, inf, h->d_A, h->stream);
     inf.mode = 4;
     inf.A = h->d_A;
-    inf.imgcode = h->d_imgcode;
   }
   if (!launched(h, k, "ewald rows")) return 3;
   if (h->a_mode != 2 || memcmp(&inf, &h->inf, sizeof(Influence)) != 0) h->version++;  // kernel arguments changed

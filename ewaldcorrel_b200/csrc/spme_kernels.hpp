@@ -101,27 +101,26 @@ struct InfConst {
 };
 
 // Influence function source for the convolution.
-// Mode 4 is mode 2 with a compact per-mode table: A (FP64) and the lattice
-// shift of the mode's single image inside the cutoff sphere (imgcode), from
-// which dA follows without evaluating f again; modes with several images
-// use mode 2's row tables.
+// Mode 4 is mode 2 with a compact per-mode table (one double per mode: A
+// with the lattice shift of the mode's single image inside the cutoff sphere
+// in its lowest mantissa bits, 0 for no image, -1 for several), from which
+// dA follows without evaluating f again; modes with several images use mode
+// 2's row tables.
 struct Influence {
   int mode;                // 1: FP64 tables A/dA; 2: Ewald on the device; 4: mode 2 + compact table
-  const double *A;         // mode 1, 4: K0*K1*ldim
+  const double *A;         // mode 1: K0*K1*ldim tables; mode 4: the packed compact table
   const double *dA;        // mode 1: 6*K0*K1*ldim
   const InfConst *ic;      // mode 2, 4: device constants
   const RowImg *rows;      // mode 2, 4: K0*K1 row image tables (rebuilt when the function is set)
-  const uint8_t *imgcode;  // mode 4: kImgNone, kImgMany, or (si+2) | (sj+2) << 2 | (sk+2) << 4
   FastDiv K2d;             // division by K2
 };
-constexpr uint8_t kImgNone = 0xFE, kImgMany = 0xFF;
 // Builds the row image tables of an Ewald influence function (mode 2).
 int launch_ewald_rows(const Geom &g, const Influence &inf, RowImg *rows, cudaStream_t st);
 // Tabulates a mode-2 influence function as FP64 tables A (nmodes) and dA
 // (6 per mode), the layout of mode 1.
 int launch_ewald_table(const Geom &g, const Influence &inf, double *A, double *dA, cudaStream_t st);
-// Compact table of a mode-2 Ewald influence function (mode 4): A and imgcode.
-int launch_ewald_compact(const Geom &g, const Influence &inf, double *A, uint8_t *imgcode, cudaStream_t st);
+// Compact table of a mode-2 Ewald influence function (mode 4), packed per mode.
+int launch_ewald_compact(const Geom &g, const Influence &inf, double *A, cudaStream_t st);
 // Tables A / dA (mode 1 layout) of a caller-sampled radial function f, f'
 // at m^2 = k dm2 (k < nt), over set_A's image set within ic.max_m.
 int launch_radial_table(const Geom &g, const InfConst &ic, const double *f, const double *df, int nt, double dm2,
