@@ -303,7 +303,7 @@ def real_space(L, x, q, eta, rcut):
 def sk_radial(L, K, acc, nbins, kmax):
     """FP64 restatement of the radial binning of a sum of |S|^2 over the
     stored half-space modes (the reference's plot.py:9-32, on the general
-    box): |k| = 2 pi |m|, m = iL^T n with n the signed x/y frequency indices
+    box): |k| = 2 pi |m|, m = inv(box) n with n the signed x/y frequency indices
     and the stored z index; bin floor(|k| / dk), dk = kmax / nbins; returns
     per-bin (sums, counts).  plot.py folds the stored z index as if that axis
     had ldim points (index >= ldim/2 taken as negative); this restatement, like
