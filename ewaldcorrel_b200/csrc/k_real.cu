@@ -14,15 +14,32 @@
 //
 // Layout: the points are cell-sorted on a coarse grid whose cells are at
 // least rcut/kRealSub wide (the same counting sort as the charge grid's, with
-// coarse dimensions), then one thread per sorted point visits the points of
-// the (2 kRealSub + 1)^3 neighbouring coarse cells (every cell of an axis
-// with fewer): for each (x, y) neighbour row the z cells are one contiguous
-// run of the sorted order.  Every pair is visited from both sides, so each
-// point's gradient has one writer and no atomics are needed; energy and
-// virial are reduced per block in FP64, then in a fixed order
-// (deterministic).  Separations come from the integer cell offsets plus the
-// FP32 in-cell fractions of the sort (about 1e-7 nm for pairs within the
-// cutoff); pair terms are FP32 (erfc, exp); all sums are FP64.
+// coarse dimensions).  One warp takes 32 consecutive sorted points; the
+// points of one coarse row (x, y cell) share their neighbourhood, so the warp
+// walks, once for all its lanes, the union of their neighbour cells: the
+// (2 kRealSub + 1)^2 neighbour rows (every row of an axis with fewer cells),
+// each a contiguous z run [zlo - kRealSub, zhi + kRealSub] of the sorted
+// order (zlo, zhi: the lanes' own z cells; the whole row when that run would
+// wrap onto itself).  A warp whose points span several rows takes the rows
+// one at a time with the other lanes masked.
+//
+// The candidates are concatenated into one stream and staged 32 at a time in
+// shared memory (x, y in cell units relative to the warp's row, the z
+// fraction and charge as a float4; the z cell relative to the warp's lowest z
+// cell as a separate exact integer), read by broadcast: a reject pass over the 32
+// computes every lane's separation and builds its 32-bit mask of pairs inside
+// the cutoff, then each lane evaluates its accepted pairs one per round
+// (erfc, exp), so the costly part runs on full lanes instead of on the few
+// lanes a candidate happens to be near.  Every pair is visited from both
+// sides, so each point's gradient has one writer and no atomics are needed.
+// Pair terms are FP32; each pair's energy is added in FP64 (the energy is a
+// sum of terms of both signs that cancels to a small fraction of their
+// magnitudes), gradient and virial terms are summed per 32-candidate chunk in
+// FP32 and added to FP64 accumulators per chunk; energy and virial are
+// reduced per block in FP64, then in a fixed order (deterministic).  Separations are
+// integer cell offsets plus the FP32 in-cell fractions of the sort (about
+// 1e-7 cells).  Pairs at zero separation (a point with itself, or two points
+// at the same position) are skipped.
 #include <cmath>
 
 #include "reduce.cuh"
@@ -31,6 +48,7 @@
 namespace spme {
 
 constexpr int kRealWords = 16;  // per-block partials: e, W[6], q^2, q, pad
+constexpr int kRealWarps = 4;   // warps per block of the pair kernel
 
 
 // Coarse cell of every sorted point, packed c0 | c1 << 10 | c2 << 20.
@@ -45,120 +63,239 @@ __global__ void __launch_bounds__(256) real_prep_kernel(int n, const uint32_t *_
 
 struct RealArgs {
   int n, nb0, nb1, nb2;
-  float inv0, inv1, inv2;         // 1 / nb
-  float ax, by, cz, bx, cx, cy;   // lattice vectors a = (ax,0,0), b = (bx,by,0), c = (cx,cy,cz)
+  float inv0, inv1, inv2;        // 1 / nb
+  float ax, by, cz, bx, cx, cy;  // lattice vectors per cell: a/nb0 = (ax,0,0), b/nb1 = (bx,by,0), c/nb2 = (cx,cy,cz)
   float eta, rc2;
-  const float4 *rec;              // in-cell fractions (cells), charge; sorted
-  const int *cellc;               // packed coarse cell; sorted
+  const float4 *rec;             // in-cell fractions (cells), charge; sorted
+  const int *cellc;              // packed coarse cell; sorted
   const uint32_t *perm;
-  const double *w;                // FP64 charges, input order (self and background sums)
+  const double *w;               // FP64 charges, input order (self and background sums)
   const int *cs;
-  double *dx;                     // dE/dx in input order (n x 3), may be null
-  double *partials;               // kRealWords per block
+  double *dx;                    // dE/dx in input order (n x 3), may be null
+  double *partials;              // kRealWords per block
 };
 
 __device__ __forceinline__ int wrapc(int c, int nb) { return c < 0 ? c + nb : (c >= nb ? c - nb : c); }
 
-// Cells of one axis to visit around cell c: [c - kRealSub, c + kRealSub] when
-// the axis has at least 2 kRealSub + 1 cells (all distinct), else every cell.
-struct AxisRange {
-  int lo, hi;  // inclusive offsets (relative when `rel`, absolute cells otherwise)
-  bool rel;
+// Per-lane state of the pair walk.
+struct RealLane {
+  float fx, fy, fz;  // own in-cell fractions
+  float oz;          // own z cell relative to the warp's lowest z cell (exact small integer)
+  float q;
+  float g0, g1, g2, w[6];          // FP32 partial sums of the current chunk
+  double E, G0, G1, G2, W[6];      // FP64 totals (E: every pair, in FP64)
 };
-__device__ __forceinline__ AxisRange axis_range(int nb) {
-  return nb >= 2 * kRealSub + 1 ? AxisRange{-kRealSub, kRealSub, true} : AxisRange{0, nb - 1, false};
+
+// Minimum-image separation (cell units) of a staged candidate from lane L;
+// WRAP reduces every axis modulo its cell count (axes with fewer than
+// 2 kRealSub + 1 cells, or a z run that covers the whole row).
+template <bool WRAP>
+__device__ __forceinline__ float pair_r2(const RealArgs &A, const RealLane &L, float4 c, float cz, float &dxv,
+                                         float &dyv, float &dzv) {
+  // integer cell offset plus the difference of two in-cell fractions: exact
+  // to the fractions' rounding for close pairs
+  float t0 = c.x - L.fx, t1 = c.y - L.fy, t2 = (cz - L.oz) + (c.z - L.fz);
+  if (WRAP) {
+    t0 -= (float)A.nb0 * rintf(t0 * A.inv0);
+    t1 -= (float)A.nb1 * rintf(t1 * A.inv1);
+    t2 -= (float)A.nb2 * rintf(t2 * A.inv2);
+  }
+  dxv = t0 * A.ax + t1 * A.bx + t2 * A.cx;
+  dyv = t1 * A.by + t2 * A.cy;
+  dzv = t2 * A.cz;
+  return dxv * dxv + dyv * dyv + dzv * dzv;
 }
 
-__global__ void __launch_bounds__(256) real_pair_kernel(RealArgs A) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[9];
+// One staged chunk of 32 candidates: the reject pass, then the accepted pairs
+// one per round.  `live`: the candidates of the chunk this lane takes (none
+// for a lane outside the current row, none past the stream's end).
+template <bool WRAP>
+__device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const float4 *__restrict__ cand,
+                                           const float *__restrict__ candz, unsigned live) {
+  unsigned mask = 0;
+#pragma unroll 8
+  for (int k = 0; k < 32; k++) {
+    float dxv, dyv, dzv;
+    const float r2 = pair_r2<WRAP>(A, L, cand[k], candz[k], dxv, dyv, dzv);
+    mask |= (r2 < A.rc2 && r2 > 0.f) ? (1u << k) : 0u;
+  }
+  mask &= live;
+  const float two_eta_sqrtpi = 1.1283791670955126f * A.eta;  // 2 eta / sqrt(pi)
+  const float eta2 = A.eta * A.eta;
+  while (mask) {
+    const int k = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const float4 c = cand[k];
+    float dxv, dyv, dzv;
+    const float r2 = pair_r2<WRAP>(A, L, c, candz[k], dxv, dyv, dzv);
+    const float ir = rsqrtf(r2);
+    const float r = r2 * ir;
+    const float phi = erfcf(A.eta * r) * ir;                              // erfc(eta r) / r
+    const float t = -L.q * c.w * (two_eta_sqrtpi * expf(-eta2 * r2) + phi) * ir * ir;  // q q phi'(r) / r
+    L.E += (double)(L.q * c.w * phi);
+    L.g0 -= t * dxv;
+    L.g1 -= t * dyv;
+    L.g2 -= t * dzv;
+    L.w[0] += t * dxv * dxv;
+    L.w[1] += t * dyv * dyv;
+    L.w[2] += t * dzv * dzv;
+    L.w[3] += t * dyv * dxv;
+    L.w[4] += t * dzv * dxv;
+    L.w[5] += t * dzv * dyv;
+  }
+  // chunk partials into the FP64 totals (each pair is visited from both
+  // sides: half of the virial; the energy is halved at the end)
+  L.G0 += (double)L.g0;
+  L.G1 += (double)L.g1;
+  L.G2 += (double)L.g2;
 #pragma unroll
-  for (int k = 0; k < 9; k++) acc[k] = 0.0;
-  if (i < A.n) {
-    const float4 ri = A.rec[i];
+  for (int k = 0; k < 6; k++) L.W[k] += 0.5 * (double)L.w[k];
+  L.g0 = L.g1 = L.g2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) L.w[k] = 0.f;
+}
+
+__global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) {
+  __shared__ float4 cand_all[kRealWarps][32];
+  __shared__ float candz_all[kRealWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float4 *cand = cand_all[warp];
+  float *candz = candz_all[warp];
+  const int i = (blockIdx.x * kRealWarps + warp) * 32 + lane;
+  const bool valid = i < A.n;
+  float4 ri = make_float4(0.f, 0.f, 0.f, 0.f);
+  int c0 = 0, c1 = 0, c2 = 0, rowi = -1;
+  if (valid) {
+    ri = A.rec[i];
     const int pi = A.cellc[i];
-    const int c0 = pi & 1023, c1 = (pi >> 10) & 1023, c2 = pi >> 20;
-    const AxisRange R0 = axis_range(A.nb0), R1 = axis_range(A.nb1), R2 = axis_range(A.nb2);
-    const float two_eta_sqrtpi = 1.1283791670955126f * A.eta;  // 2 eta / sqrt(pi)
-    const float eta2 = A.eta * A.eta;
-    double e = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, W[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    // one contiguous run of sorted points
-    auto run = [&](int j0, int j1) {
-      for (int j = j0; j < j1; j++) {
-        if (j == i) continue;
-        const float4 rj = A.rec[j];
-        const int pj = A.cellc[j];
-        // minimum-image separation in cells: integer cell difference plus the
-        // in-cell fractions, reduced modulo the axis (exact for the small
-        // differences of pairs within the cutoff)
-        float t0 = (float)((pj & 1023) - c0) + (rj.x - ri.x);
-        float t1 = (float)(((pj >> 10) & 1023) - c1) + (rj.y - ri.y);
-        float t2 = (float)((pj >> 20) - c2) + (rj.z - ri.z);
-        t0 -= (float)A.nb0 * rintf(t0 * A.inv0);
-        t1 -= (float)A.nb1 * rintf(t1 * A.inv1);
-        t2 -= (float)A.nb2 * rintf(t2 * A.inv2);
-        const float s0 = t0 * A.inv0, s1 = t1 * A.inv1, s2 = t2 * A.inv2;
-        const float dxv = s0 * A.ax + s1 * A.bx + s2 * A.cx;
-        const float dyv = s1 * A.by + s2 * A.cy;
-        const float dzv = s2 * A.cz;
-        const float r2 = dxv * dxv + dyv * dyv + dzv * dzv;
-        if (r2 >= A.rc2) continue;
-        const float r = sqrtf(r2), ir = 1.f / r;
-        const float ec = erfcf(A.eta * r);
-        const float phi = ec * ir;                                           // erfc(eta r) / r
-        const float dphi = -(two_eta_sqrtpi * expf(-eta2 * r2) + phi) * ir;  // d phi / dr
-        const float qq = ri.w * rj.w;
-        e += 0.5 * (double)(qq * phi);
-        const float t = qq * dphi * ir;  // q q phi'(r) / r
-        g0 -= (double)(t * dxv);
-        g1 -= (double)(t * dyv);
-        g2 -= (double)(t * dzv);
-        const float h = 0.5f * t;  // each pair is visited from both sides
-        W[0] += (double)(h * dxv * dxv);
-        W[1] += (double)(h * dyv * dyv);
-        W[2] += (double)(h * dzv * dzv);
-        W[3] += (double)(h * dyv * dxv);
-        W[4] += (double)(h * dzv * dxv);
-        W[5] += (double)(h * dzv * dyv);
-      }
-    };
-    for (int d0 = R0.lo; d0 <= R0.hi; d0++) {
-      const int n0 = R0.rel ? wrapc(c0 + d0, A.nb0) : d0;
-      for (int d1 = R1.lo; d1 <= R1.hi; d1++) {
-        const int n1 = R1.rel ? wrapc(c1 + d1, A.nb1) : d1;
-        const long row = ((long)n0 * A.nb1 + n1) * A.nb2;
-        if (!R2.rel) {
-          run(A.cs[row], A.cs[row + A.nb2]);  // the whole row
+    c0 = pi & 1023;
+    c1 = (pi >> 10) & 1023;
+    c2 = pi >> 20;
+    rowi = (c0 << 10) | c1;
+  }
+  RealLane L;
+  L.fx = ri.x;
+  L.fy = ri.y;
+  L.q = ri.w;
+  L.g0 = L.g1 = L.g2 = 0.f;
+  L.E = L.G0 = L.G1 = L.G2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    L.w[k] = 0.f;
+    L.W[k] = 0.0;
+  }
+  const bool rel0 = A.nb0 >= 2 * kRealSub + 1, rel1 = A.nb1 >= 2 * kRealSub + 1;
+  const int n0r = rel0 ? 2 * kRealSub + 1 : A.nb0, n1r = rel1 ? 2 * kRealSub + 1 : A.nb1;
+  const int nrows = n0r * n1r;  // <= 25: one lane per neighbour row
+  unsigned todo = __ballot_sync(0xffffffffu, valid);
+  while (todo) {
+    const int row = __shfl_sync(0xffffffffu, rowi, __ffs(todo) - 1);
+    const bool act = rowi == row;
+    todo &= ~__ballot_sync(0xffffffffu, act);
+    const int rc0 = row >> 10, rc1 = row & 1023;
+    const int zlo = __reduce_min_sync(0xffffffffu, act ? c2 : 0x7fffffff);
+    const int zhi = __reduce_max_sync(0xffffffffu, act ? c2 : -1);
+    const bool wholez = zhi - zlo + 2 * kRealSub + 1 >= A.nb2;
+    const bool wrap = !rel0 || !rel1 || wholez;
+    L.fz = ri.z;
+    L.oz = (float)(c2 - zlo);
+    // this lane's neighbour row: offsets, pieces [s1, s1 + l1) and [s2, s2 + l2)
+    // of the sorted order, with the z cell shifts that unwrap them
+    int s1 = 0, l1 = 0, sh1 = 0, s2 = 0, l2 = 0, sh2 = 0;
+    float o0 = 0.f, o1 = 0.f;
+    if (lane < nrows) {
+      const int r0 = lane / n1r, r1 = lane - r0 * n1r;
+      const int nn0 = rel0 ? wrapc(rc0 + r0 - kRealSub, A.nb0) : r0;
+      const int nn1 = rel1 ? wrapc(rc1 + r1 - kRealSub, A.nb1) : r1;
+      o0 = (float)(rel0 ? r0 - kRealSub : r0 - rc0);
+      o1 = (float)(rel1 ? r1 - kRealSub : r1 - rc1);
+      const long rb = ((long)nn0 * A.nb1 + nn1) * A.nb2;
+      if (wholez) {
+        s1 = A.cs[rb];
+        l1 = A.cs[rb + A.nb2] - s1;
+      } else {
+        const int za = zlo - kRealSub, zb = zhi + kRealSub;
+        if (za < 0) {
+          s1 = A.cs[rb + za + A.nb2];
+          l1 = A.cs[rb + A.nb2] - s1;
+          sh1 = -A.nb2;
+          s2 = A.cs[rb];
+          l2 = A.cs[rb + zb + 1] - s2;
+        } else if (zb >= A.nb2) {
+          s1 = A.cs[rb + za];
+          l1 = A.cs[rb + A.nb2] - s1;
+          s2 = A.cs[rb];
+          l2 = A.cs[rb + zb + 1 - A.nb2] - s2;
+          sh2 = A.nb2;
         } else {
-          // z cells c2 - Sub .. c2 + Sub: contiguous in the sorted order, in at
-          // most two pieces when they wrap
-          const int za = c2 - kRealSub, zb = c2 + kRealSub;
-          if (za < 0) {
-            run(A.cs[row + za + A.nb2], A.cs[row + A.nb2]);
-            run(A.cs[row], A.cs[row + zb + 1]);
-          } else if (zb >= A.nb2) {
-            run(A.cs[row + za], A.cs[row + A.nb2]);
-            run(A.cs[row], A.cs[row + zb + 1 - A.nb2]);
-          } else {
-            run(A.cs[row + za], A.cs[row + zb + 1]);
-          }
+          s1 = A.cs[rb + za];
+          l1 = A.cs[rb + zb + 1] - s1;
         }
       }
     }
+    // exclusive prefix of the rows' candidate counts
+    int pre = l1 + l2;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, pre, 31);
+    pre -= l1 + l2;
+    for (int v0 = 0; v0 < total; v0 += 32) {
+      const int v = v0 + lane;
+      float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);  // past the end: masked out below
+      float cvz = 0.f;
+      // row of stream position v: the last row whose prefix is <= v
+      int r = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int pr = __shfl_sync(0xffffffffu, pre, r + step < nrows ? r + step : r);
+        if (r + step < nrows && pr <= v) r += step;
+      }
+      const int rs1 = __shfl_sync(0xffffffffu, s1, r), rl1 = __shfl_sync(0xffffffffu, l1, r);
+      const int rs2 = __shfl_sync(0xffffffffu, s2, r), rsh1 = __shfl_sync(0xffffffffu, sh1, r);
+      const int rsh2 = __shfl_sync(0xffffffffu, sh2, r), rpre = __shfl_sync(0xffffffffu, pre, r);
+      const float ro0 = __shfl_sync(0xffffffffu, o0, r), ro1 = __shfl_sync(0xffffffffu, o1, r);
+      if (v < total) {
+        const int loc = v - rpre;
+        const int j = loc < rl1 ? rs1 + loc : rs2 + (loc - rl1);
+        const int sh = loc < rl1 ? rsh1 : rsh2;
+        const float4 rj = A.rec[j];
+        const int cz = A.cellc[j] >> 20;
+        cv = make_float4(ro0 + rj.x, ro1 + rj.y, rj.z, rj.w);
+        cvz = (float)(cz + sh - zlo);
+      }
+      __syncwarp();
+      cand[lane] = cv;
+      candz[lane] = cvz;
+      __syncwarp();
+      const int cnt = total - v0;
+      const unsigned live = act ? (cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u) : 0u;
+      if (wrap)
+        real_chunk<true>(A, L, cand, candz, live);
+      else
+        real_chunk<false>(A, L, cand, candz, live);
+    }
+  }
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) acc[k] = 0.0;
+  if (valid) {
     const int a = (int)A.perm[i];
     if (A.dx) {
-      A.dx[3 * a] = g0;
-      A.dx[3 * a + 1] = g1;
-      A.dx[3 * a + 2] = g2;
+      A.dx[3 * a] = L.G0;
+      A.dx[3 * a + 1] = L.G1;
+      A.dx[3 * a + 2] = L.G2;
     }
-    acc[0] = e;
+    acc[0] = 0.5 * L.E;
 #pragma unroll
-    for (int k = 0; k < 6; k++) acc[1 + k] = W[k];
+    for (int k = 0; k < 6; k++) acc[1 + k] = L.W[k];
     const double q = A.w[a];
     acc[7] = q * q;
     acc[8] = q;
   }
-  __shared__ double red[8][9];
+  __shared__ double red[kRealWarps][9];
   block_reduce_n<9>(acc, red, A.partials + (long)blockIdx.x * kRealWords);
 }
 
@@ -179,16 +316,18 @@ __global__ void real_finish_kernel(const double *__restrict__ partials, int nblo
   out[9] = -pi * tot[8] * tot[8] * iV * iV / (2.0 * eta * eta);
 }
 
-size_t real_partial_words(int cap) { return (size_t)((cap + 255) / 256 + 1) * kRealWords; }
+size_t real_partial_words(int cap) {
+  return (size_t)((cap + kRealWarps * 32 - 1) / (kRealWarps * 32) + 1) * kRealWords;
+}
 
 int launch_real_space(const Geom &coarse, const double L[6], int n, const double *x, const double *w, float eta,
                       float rcut, SortBuffers &sb, double4 *rec, double *dx, double *partials, double eta_d,
                       double *out, cudaStream_t st) {
   int k = launch_cell_sort(coarse, n, x, w, sb, st);
-  const int blocks = (n + 255) / 256;
+  const int blocks = (n + kRealWarps * 32 - 1) / (kRealWarps * 32);
   if (n > 0) {
     int *cellc = reinterpret_cast<int *>(rec);  // rec holds n ints here
-    real_prep_kernel<<<blocks, 256, 0, st>>>(n, sb.keys[sb.cur], coarse.K1, coarse.K2, cellc);
+    real_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, sb.keys[sb.cur], coarse.K1, coarse.K2, cellc);
     RealArgs A{};
     A.n = n;
     A.nb0 = coarse.K0;
@@ -197,12 +336,12 @@ int launch_real_space(const Geom &coarse, const double L[6], int n, const double
     A.inv0 = 1.f / (float)coarse.K0;
     A.inv1 = 1.f / (float)coarse.K1;
     A.inv2 = 1.f / (float)coarse.K2;
-    A.ax = (float)L[0];
-    A.by = (float)L[1];
-    A.cz = (float)L[2];
-    A.bx = (float)L[3];
-    A.cx = (float)L[4];
-    A.cy = (float)L[5];
+    A.ax = (float)(L[0] / coarse.K0);
+    A.by = (float)(L[1] / coarse.K1);
+    A.cz = (float)(L[2] / coarse.K2);
+    A.bx = (float)(L[3] / coarse.K1);
+    A.cx = (float)(L[4] / coarse.K2);
+    A.cy = (float)(L[5] / coarse.K2);
     A.eta = eta;
     A.rc2 = rcut * rcut;
     A.rec = sb.rec_sorted;
@@ -212,7 +351,7 @@ int launch_real_space(const Geom &coarse, const double L[6], int n, const double
     A.cs = sb.cell_start;
     A.dx = dx;
     A.partials = partials;
-    real_pair_kernel<<<blocks, 256, 0, st>>>(A);
+    real_pair_kernel<<<blocks, kRealWarps * 32, 0, st>>>(A);
     k += 2;
   }
   real_finish_kernel<<<1, 9 * 32, 0, st>>>(partials, blocks, coarse.cell, eta_d, out);
