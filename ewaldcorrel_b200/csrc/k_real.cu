@@ -32,6 +32,15 @@
 // (erfc, exp), so the costly part runs on full lanes instead of on the few
 // lanes a candidate happens to be near.  Every pair is visited from both
 // sides, so each point's gradient has one writer and no atomics are needed.
+// Warps take their 32-point groups from a counter (groups differ in work:
+// one or more rows, longer or shorter z runs), and every group writes its own
+// energy / virial partials, summed in group order afterwards, so the result
+// does not depend on which warp took which group.
+//
+// erfc(x) = exp(-x^2) erfcx(x): the exponential is the one the gradient needs
+// anyway, and erfcx (smooth, between 1 and about 1/(x sqrt(pi))) is a
+// cubic-Hermite table of kRealTab intervals on [0, min(eta rcut, 10)] built
+// in FP64 per call and read from shared memory.
 // Pair terms are FP32; each pair's energy is added in FP64 (the energy is a
 // sum of terms of both signs that cancels to a small fraction of their
 // magnitudes), gradient and virial terms are summed per 32-candidate chunk in
@@ -40,6 +49,7 @@
 // integer cell offsets plus the FP32 in-cell fractions of the sort (about
 // 1e-7 cells).  Pairs at zero separation (a point with itself, or two points
 // at the same position) are skipped.
+#include <algorithm>
 #include <cmath>
 
 #include "reduce.cuh"
@@ -47,14 +57,30 @@
 
 namespace spme {
 
-constexpr int kRealWords = 16;  // per-block partials: e, W[6], q^2, q, pad
+constexpr int kRealWords = 16;  // per-group partials: e, W[6], q^2, q, pad
 constexpr int kRealWarps = 4;   // warps per block of the pair kernel
+constexpr int kRealBlocksPerSM = 7;
+
+// Cubic-Hermite table of erfcx(x) = exp(x^2) erfc(x) on [0, xmax]: interval
+// k holds f(k h + t h) = c.x + t (c.y + t (c.z + t c.w)), t in [0, 1].
+__global__ void real_table_kernel(int ntab, double xmax, float4 *__restrict__ tab) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ntab) return;
+  const double h = xmax / ntab, x0 = k * h, x1 = x0 + h;
+  const double two_rsqrtpi = 1.1283791670955126;  // 2 / sqrt(pi)
+  const double f0 = erfc(x0) * exp(x0 * x0), f1 = erfc(x1) * exp(x1 * x1);
+  const double d0 = (2.0 * x0 * f0 - two_rsqrtpi) * h, d1 = (2.0 * x1 * f1 - two_rsqrtpi) * h;  // f' h
+  tab[k] = make_float4((float)f0, (float)d0, (float)(3.0 * (f1 - f0) - 2.0 * d0 - d1),
+                       (float)(2.0 * (f0 - f1) + d0 + d1));
+}
 
 
-// Coarse cell of every sorted point, packed c0 | c1 << 10 | c2 << 20.
+// Coarse cell of every sorted point, packed c0 | c1 << 10 | c2 << 20; zeroes
+// the pair kernel's group counter.
 __global__ void __launch_bounds__(256) real_prep_kernel(int n, const uint32_t *__restrict__ keys, int nb1, int nb2,
-                                                        int *__restrict__ cellc) {
+                                                        int *__restrict__ cellc, int *__restrict__ next) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *next = 0;
   if (i >= n) return;
   const uint32_t key = keys[i];
   const int c2 = (int)(key % (uint32_t)nb2), r = (int)(key / (uint32_t)nb2);
@@ -66,13 +92,17 @@ struct RealArgs {
   float inv0, inv1, inv2;        // 1 / nb
   float ax, by, cz, bx, cx, cy;  // lattice vectors per cell: a/nb0 = (ax,0,0), b/nb1 = (bx,by,0), c/nb2 = (cx,cy,cz)
   float eta, rc2;
+  float tab_scale;               // erfcx table intervals per unit x
+  int ngroups;                   // 32-point groups
+  int *next;                     // group counter (zeroed by real_prep_kernel)
+  const float4 *tab;             // erfcx table (kRealTab intervals)
   const float4 *rec;             // in-cell fractions (cells), charge; sorted
   const int *cellc;              // packed coarse cell; sorted
   const uint32_t *perm;
   const double *w;               // FP64 charges, input order (self and background sums)
   const int *cs;
   double *dx;                    // dE/dx in input order (n x 3), may be null
-  double *partials;              // kRealWords per block
+  double *partials;              // kRealWords per group
 };
 
 __device__ __forceinline__ int wrapc(int c, int nb) { return c < 0 ? c + nb : (c >= nb ? c - nb : c); }
@@ -111,13 +141,14 @@ __device__ __forceinline__ float pair_r2(const RealArgs &A, const RealLane &L, f
 // for a lane outside the current row, none past the stream's end).
 template <bool WRAP>
 __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const float4 *__restrict__ cand,
-                                           const float *__restrict__ candz, unsigned live) {
+                                           const float *__restrict__ candz, const float4 *__restrict__ tab,
+                                           unsigned live) {
   unsigned mask = 0;
 #pragma unroll 8
   for (int k = 0; k < 32; k++) {
     float dxv, dyv, dzv;
     const float r2 = pair_r2<WRAP>(A, L, cand[k], candz[k], dxv, dyv, dzv);
-    mask |= (r2 < A.rc2 && r2 > 0.f) ? (1u << k) : 0u;
+    mask |= (r2 < A.rc2) ? (1u << k) : 0u;  // zero separations are dropped below
   }
   mask &= live;
   const float two_eta_sqrtpi = 1.1283791670955126f * A.eta;  // 2 eta / sqrt(pi)
@@ -128,11 +159,18 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
     const float4 c = cand[k];
     float dxv, dyv, dzv;
     const float r2 = pair_r2<WRAP>(A, L, c, candz[k], dxv, dyv, dzv);
+    if (r2 == 0.f) continue;  // the point itself (or a coincident one)
     const float ir = rsqrtf(r2);
-    const float r = r2 * ir;
-    const float phi = erfcf(A.eta * r) * ir;                              // erfc(eta r) / r
-    const float t = -L.q * c.w * (two_eta_sqrtpi * expf(-eta2 * r2) + phi) * ir * ir;  // q q phi'(r) / r
-    L.E += (double)(L.q * c.w * phi);
+    const float ex = expf(-eta2 * r2);  // exp(-x^2), x = eta r
+    const float u = A.eta * (r2 * ir) * A.tab_scale;
+    const int ti = min((int)u, kRealTab - 1);
+    const float tt = fminf(u - (float)ti, 1.f);
+    const float4 cf = tab[ti];
+    const float erfcx = fmaf(tt, fmaf(tt, fmaf(tt, cf.w, cf.z), cf.y), cf.x);
+    const float phi = ex * erfcx * ir;  // erfc(eta r) / r
+    const float qq = L.q * c.w;
+    const float t = -qq * (two_eta_sqrtpi * ex + phi) * ir * ir;  // q q phi'(r) / r
+    L.E += (double)(qq * phi);
     L.g0 -= t * dxv;
     L.g1 -= t * dyv;
     L.g2 -= t * dzv;
@@ -155,13 +193,12 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
   for (int k = 0; k < 6; k++) L.w[k] = 0.f;
 }
 
-__global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) {
-  __shared__ float4 cand_all[kRealWarps][32];
-  __shared__ float candz_all[kRealWarps][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float4 *cand = cand_all[warp];
-  float *candz = candz_all[warp];
-  const int i = (blockIdx.x * kRealWarps + warp) * 32 + lane;
+// One 32-point group of sorted points per warp at a time, taken from the
+// group counter; writes the group's partials.
+__device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *cand, float *candz,
+                                           const float4 *tab) {
+  const int lane = threadIdx.x & 31;
+  const int i = grp * 32 + lane;
   const bool valid = i < A.n;
   float4 ri = make_float4(0.f, 0.f, 0.f, 0.f);
   int c0 = 0, c1 = 0, c2 = 0, rowi = -1;
@@ -273,9 +310,9 @@ __global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) 
       const int cnt = total - v0;
       const unsigned live = act ? (cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u) : 0u;
       if (wrap)
-        real_chunk<true>(A, L, cand, candz, live);
+        real_chunk<true>(A, L, cand, candz, tab, live);
       else
-        real_chunk<false>(A, L, cand, candz, live);
+        real_chunk<false>(A, L, cand, candz, tab, live);
     }
   }
   double acc[9];
@@ -295,8 +332,27 @@ __global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) 
     acc[7] = q * q;
     acc[8] = q;
   }
-  __shared__ double red[kRealWarps][9];
-  block_reduce_n<9>(acc, red, A.partials + (long)blockIdx.x * kRealWords);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const double v = warp_sum(acc[k]);
+    if (lane == k) A.partials[(long)grp * kRealWords + k] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) {
+  __shared__ float4 cand_all[kRealWarps][32];
+  __shared__ float candz_all[kRealWarps][32];
+  __shared__ float4 tab[kRealTab];
+  for (int k = threadIdx.x; k < kRealTab; k += blockDim.x) tab[k] = A.tab[k];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    int grp = 0;
+    if (lane == 0) grp = atomicAdd(A.next, 1);
+    grp = __shfl_sync(0xffffffffu, grp, 0);
+    if (grp >= A.ngroups) break;
+    real_group(A, grp, cand_all[warp], candz_all[warp], tab);
+  }
 }
 
 // out = [E_real, E_self, E_net, vir_real (xx, yy, zz, yx, zx, zy), vir_net
@@ -316,18 +372,19 @@ __global__ void real_finish_kernel(const double *__restrict__ partials, int nblo
   out[9] = -pi * tot[8] * tot[8] * iV * iV / (2.0 * eta * eta);
 }
 
-size_t real_partial_words(int cap) {
-  return (size_t)((cap + kRealWarps * 32 - 1) / (kRealWarps * 32) + 1) * kRealWords;
-}
+size_t real_partial_words(int cap) { return (size_t)((cap + 31) / 32 + 1) * kRealWords; }
 
 int launch_real_space(const Geom &coarse, const double L[6], int n, const double *x, const double *w, float eta,
-                      float rcut, SortBuffers &sb, double4 *rec, double *dx, double *partials, double eta_d,
-                      double *out, cudaStream_t st) {
+                      float rcut, SortBuffers &sb, double4 *rec, float4 *tab, double *dx, double *partials,
+                      double eta_d, double *out, cudaStream_t st) {
   int k = launch_cell_sort(coarse, n, x, w, sb, st);
-  const int blocks = (n + kRealWarps * 32 - 1) / (kRealWarps * 32);
+  const int ngroups = (n + 31) / 32;
   if (n > 0) {
     int *cellc = reinterpret_cast<int *>(rec);  // rec holds n ints here
-    real_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, sb.keys[sb.cur], coarse.K1, coarse.K2, cellc);
+    int *next = reinterpret_cast<int *>(partials + (size_t)ngroups * kRealWords);  // past the group records
+    real_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, sb.keys[sb.cur], coarse.K1, coarse.K2, cellc, next);
+    const double xmax = fmin(eta_d * (double)rcut, 10.0);  // exp(-x^2) is 0 in FP32 beyond x = 10
+    real_table_kernel<<<(kRealTab + 127) / 128, 128, 0, st>>>(kRealTab, xmax, tab);
     RealArgs A{};
     A.n = n;
     A.nb0 = coarse.K0;
@@ -344,6 +401,10 @@ int launch_real_space(const Geom &coarse, const double L[6], int n, const double
     A.cy = (float)(L[5] / coarse.K2);
     A.eta = eta;
     A.rc2 = rcut * rcut;
+    A.tab_scale = (float)(kRealTab / xmax);
+    A.ngroups = ngroups;
+    A.next = next;
+    A.tab = tab;
     A.rec = sb.rec_sorted;
     A.cellc = cellc;
     A.perm = sb.vals[sb.cur];
@@ -351,10 +412,14 @@ int launch_real_space(const Geom &coarse, const double L[6], int n, const double
     A.cs = sb.cell_start;
     A.dx = dx;
     A.partials = partials;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = std::min((ngroups + kRealWarps - 1) / kRealWarps, nsm * kRealBlocksPerSM);
     real_pair_kernel<<<blocks, kRealWarps * 32, 0, st>>>(A);
-    k += 2;
+    k += 3;
   }
-  real_finish_kernel<<<1, 9 * 32, 0, st>>>(partials, blocks, coarse.cell, eta_d, out);
+  real_finish_kernel<<<1, 9 * 32, 0, st>>>(partials, ngroups, coarse.cell, eta_d, out);
   return k + 1;
 }
 

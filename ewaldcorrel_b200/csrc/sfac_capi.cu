@@ -69,6 +69,7 @@ struct Handle {
     long ncell = 0;
     double4 *rec = nullptr;
     double *x = nullptr, *w = nullptr, *dx = nullptr, *part = nullptr, *out = nullptr;
+    float4 *tab = nullptr;  // erfcx table of the pair kernel
   } rs;
   // pipelined de2 / potl: copy-in and copy-out streams, per-chunk events
   cudaStream_t s_in = nullptr, s_out = nullptr;
@@ -197,6 +198,7 @@ void free_real(Handle *h) {
   dfree(r.dx);
   dfree(r.part);
   dfree(r.out);
+  dfree(r.tab);
   r.cap = 0;
   r.ncell = 0;
 }
@@ -212,7 +214,8 @@ bool ensure_real(Handle *h, int n, long ncell) {
   ok = ok && dalloc(h, &r.sb.tmp, cap) && dalloc(h, &r.sb.rec, cap) && dalloc(h, &r.sb.rec_sorted, cap) &&
        dalloc(h, &r.sb.hist, cap) && dalloc(h, &r.sb.cell_start, cell_count_words(ncell)) &&
        dalloc(h, &r.rec, cap) && dalloc(h, &r.x, 3 * (size_t)cap) && dalloc(h, &r.w, cap) &&
-       dalloc(h, &r.dx, 3 * (size_t)cap) && dalloc(h, &r.part, real_partial_words(cap)) && dalloc(h, &r.out, 16);
+       dalloc(h, &r.dx, 3 * (size_t)cap) && dalloc(h, &r.part, real_partial_words(cap)) && dalloc(h, &r.out, 16) &&
+       dalloc(h, &r.tab, kRealTab);
   if (!ok) {
     free_real(h);
     return false;
@@ -720,8 +723,8 @@ int sfac_real_space_device(void *p, int n, const double *x, const double *w, dou
   Geom cg;
   const int rc = real_prepare(h, n, eta, rcut, cg);
   if (rc) return rc;
-  const int k = launch_real_space(cg, h->L, n, x, w, (float)eta, (float)rcut, h->rs.sb, h->rs.rec, dx, h->rs.part,
-                                  eta, out, h->stream);
+  const int k = launch_real_space(cg, h->L, n, x, w, (float)eta, (float)rcut, h->rs.sb, h->rs.rec, h->rs.tab, dx,
+                                  h->rs.part, eta, out, h->stream);
   return launched(h, k, "real-space kernels") ? 0 : 2;
 }
 
@@ -736,7 +739,7 @@ int sfac_real_space(void *p, int n, const double *w, const double *x, double eta
                 !CK(h, cudaMemcpyAsync(h->rs.w, w, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream))))
     return 2;
   const int k = launch_real_space(cg, h->L, n, h->rs.x, h->rs.w, (float)eta, (float)rcut, h->rs.sb, h->rs.rec,
-                                  dx ? h->rs.dx : nullptr, h->rs.part, eta, h->rs.out, h->stream);
+                                  h->rs.tab, dx ? h->rs.dx : nullptr, h->rs.part, eta, h->rs.out, h->stream);
   if (!launched(h, k, "real-space kernels")) return 2;
   if (!CK(h, cudaMemcpyAsync(out, h->rs.out, sizeof(double) * 10, cudaMemcpyDeviceToHost, h->stream))) return 2;
   if (dx && n > 0 &&

@@ -164,13 +164,16 @@ int launch_xc_accumulate(long nmodes, int D, const float2 *Q, double2 *C, cudaSt
 // Coarse cells of the real-space cell list are at least rcut / kRealSub wide;
 // the pair kernel searches kRealSub cells either side.
 constexpr int kRealSub = 2;
+// Intervals of the erfcx table of the pair kernel (float4 each).
+constexpr int kRealTab = 256;
 // Cell sort of the points on the coarse grid `coarse` (cells >= rcut wide),
 // then the minimum-image erfc pair sum: dx (n x 3, input order, may be null)
 // and out (device, 10 doubles: E_real, E_self, E_net, virial[6], net-charge
-// virial diagonal).  partials: real_partial_words(n) doubles.
+// virial diagonal).  partials: real_partial_words(n) doubles; tab: kRealTab
+// float4.
 int launch_real_space(const Geom &coarse, const double L[6], int n, const double *x, const double *w, float eta,
-                      float rcut, SortBuffers &sb, double4 *rec, double *dx, double *partials, double eta_d,
-                      double *out, cudaStream_t st);
+                      float rcut, SortBuffers &sb, double4 *rec, float4 *tab, double *dx, double *partials,
+                      double eta_d, double *out, cudaStream_t st);
 size_t real_partial_words(int cap);
 
 }  // namespace spme
