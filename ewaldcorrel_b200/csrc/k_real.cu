@@ -26,9 +26,11 @@
 // The candidates are concatenated into one stream and staged 32 at a time in
 // shared memory (x, y in cell units relative to the warp's row, the z
 // fraction and charge as a float4; the z cell relative to the warp's lowest z
-// cell as a separate exact integer), read by broadcast: a reject pass over the 32
-// computes every lane's separation and builds its 32-bit mask of pairs inside
-// the cutoff, then each lane evaluates its accepted pairs one per round
+// cell as a separate exact integer; the Cartesian position relative to the
+// warp's first cell), read by broadcast: a reject pass over the 32 computes
+// every lane's distance (Cartesian, against a cutoff widened by 1e-4 of rc^2
+// to cover its rounding, when no image reduction is needed) and builds its
+// 32-bit mask of candidates inside, then each lane evaluates its accepted pairs one per round
 // (erfc, exp), so the costly part runs on full lanes instead of on the few
 // lanes a candidate happens to be near.  Every pair is visited from both
 // sides, so each point's gradient has one writer and no atomics are needed.
@@ -59,7 +61,7 @@ namespace spme {
 
 constexpr int kRealWords = 16;  // per-group partials: e, W[6], q^2, q, pad
 constexpr int kRealWarps = 4;   // warps per block of the pair kernel
-constexpr int kRealBlocksPerSM = 7;
+constexpr int kRealBlocksPerSM = 6;
 
 // Cubic-Hermite table of erfcx(x) = exp(x^2) erfc(x) on [0, xmax]: interval
 // k holds f(k h + t h) = c.x + t (c.y + t (c.z + t c.w)), t in [0, 1].
@@ -92,6 +94,7 @@ struct RealArgs {
   float inv0, inv1, inv2;        // 1 / nb
   float ax, by, cz, bx, cx, cy;  // lattice vectors per cell: a/nb0 = (ax,0,0), b/nb1 = (bx,by,0), c/nb2 = (cx,cy,cz)
   float eta, rc2;
+  float rc2l;                    // rc2 widened past the rounding of the Cartesian reject test
   float tab_scale;               // erfcx table intervals per unit x
   int ngroups;                   // 32-point groups
   int *next;                     // group counter (zeroed by real_prep_kernel)
@@ -111,6 +114,7 @@ __device__ __forceinline__ int wrapc(int c, int nb) { return c < 0 ? c + nb : (c
 struct RealLane {
   float fx, fy, fz;  // own in-cell fractions
   float oz;          // own z cell relative to the warp's lowest z cell (exact small integer)
+  float px, py, pz;  // own Cartesian position relative to the warp's row and lowest z cell
   float q;
   float g0, g1, g2, w[6];          // FP32 partial sums of the current chunk
   double E, G0, G1, G2, W[6];      // FP64 totals (E: every pair, in FP64)
@@ -141,14 +145,26 @@ __device__ __forceinline__ float pair_r2(const RealArgs &A, const RealLane &L, f
 // for a lane outside the current row, none past the stream's end).
 template <bool WRAP>
 __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const float4 *__restrict__ cand,
-                                           const float *__restrict__ candz, const float4 *__restrict__ tab,
-                                           unsigned live) {
+                                           const float *__restrict__ candz, const float4 *__restrict__ cart,
+                                           const float4 *__restrict__ tab, unsigned live) {
   unsigned mask = 0;
+  if (WRAP) {
 #pragma unroll 8
-  for (int k = 0; k < 32; k++) {
-    float dxv, dyv, dzv;
-    const float r2 = pair_r2<WRAP>(A, L, cand[k], candz[k], dxv, dyv, dzv);
-    mask |= (r2 < A.rc2) ? (1u << k) : 0u;  // zero separations are dropped below
+    for (int k = 0; k < 32; k++) {
+      float dxv, dyv, dzv;
+      const float r2 = pair_r2<WRAP>(A, L, cand[k], candz[k], dxv, dyv, dzv);
+      mask |= (r2 < A.rc2) ? (1u << k) : 0u;  // zero separations are dropped below
+    }
+  } else {
+    // no image reduction: a plain Cartesian distance against the widened
+    // cutoff; the accepted pairs are tested again from the exact separation
+#pragma unroll 8
+    for (int k = 0; k < 32; k++) {
+      const float4 p = cart[k];
+      const float ddx = p.x - L.px, ddy = p.y - L.py, ddz = p.z - L.pz;
+      const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      mask |= (r2 < A.rc2l) ? (1u << k) : 0u;
+    }
   }
   mask &= live;
   const float two_eta_sqrtpi = 1.1283791670955126f * A.eta;  // 2 eta / sqrt(pi)
@@ -159,7 +175,7 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
     const float4 c = cand[k];
     float dxv, dyv, dzv;
     const float r2 = pair_r2<WRAP>(A, L, c, candz[k], dxv, dyv, dzv);
-    if (r2 == 0.f) continue;  // the point itself (or a coincident one)
+    if (!(r2 < A.rc2) || r2 == 0.f) continue;  // outside the cutoff; the point itself (or a coincident one)
     const float ir = rsqrtf(r2);
     const float ex = expf(-eta2 * r2);  // exp(-x^2), x = eta r
     const float u = A.eta * (r2 * ir) * A.tab_scale;
@@ -195,7 +211,7 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
 
 // One 32-point group of sorted points per warp at a time, taken from the
 // group counter; writes the group's partials.
-__device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *cand, float *candz,
+__device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *cand, float *candz, float4 *cart,
                                            const float4 *tab) {
   const int lane = threadIdx.x & 31;
   const int i = grp * 32 + lane;
@@ -236,6 +252,12 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
     const bool wrap = !rel0 || !rel1 || wholez;
     L.fz = ri.z;
     L.oz = (float)(c2 - zlo);
+    {
+      const float zc = L.oz + L.fz;
+      L.px = L.fx * A.ax + L.fy * A.bx + zc * A.cx;
+      L.py = L.fy * A.by + zc * A.cy;
+      L.pz = zc * A.cz;
+    }
     // this lane's neighbour row: offsets, pieces [s1, s1 + l1) and [s2, s2 + l2)
     // of the sorted order, with the z cell shifts that unwrap them
     int s1 = 0, l1 = 0, sh1 = 0, s2 = 0, l2 = 0, sh2 = 0;
@@ -283,6 +305,7 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
       const int v = v0 + lane;
       float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);  // past the end: masked out below
       float cvz = 0.f;
+      float4 cvp = make_float4(0.f, 0.f, 0.f, 0.f);
       // row of stream position v: the last row whose prefix is <= v
       int r = 0;
 #pragma unroll
@@ -302,17 +325,20 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
         const int cz = A.cellc[j] >> 20;
         cv = make_float4(ro0 + rj.x, ro1 + rj.y, rj.z, rj.w);
         cvz = (float)(cz + sh - zlo);
+        const float zc = cvz + rj.z;
+        cvp = make_float4(cv.x * A.ax + cv.y * A.bx + zc * A.cx, cv.y * A.by + zc * A.cy, zc * A.cz, 0.f);
       }
       __syncwarp();
       cand[lane] = cv;
       candz[lane] = cvz;
+      cart[lane] = cvp;
       __syncwarp();
       const int cnt = total - v0;
       const unsigned live = act ? (cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u) : 0u;
       if (wrap)
-        real_chunk<true>(A, L, cand, candz, tab, live);
+        real_chunk<true>(A, L, cand, candz, cart, tab, live);
       else
-        real_chunk<false>(A, L, cand, candz, tab, live);
+        real_chunk<false>(A, L, cand, candz, cart, tab, live);
     }
   }
   double acc[9];
@@ -339,9 +365,10 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
   }
 }
 
-__global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) {
+__global__ void __launch_bounds__(kRealWarps * 32, kRealBlocksPerSM) real_pair_kernel(RealArgs A) {
   __shared__ float4 cand_all[kRealWarps][32];
   __shared__ float candz_all[kRealWarps][32];
+  __shared__ float4 cart_all[kRealWarps][32];
   __shared__ float4 tab[kRealTab];
   for (int k = threadIdx.x; k < kRealTab; k += blockDim.x) tab[k] = A.tab[k];
   __syncthreads();
@@ -351,7 +378,7 @@ __global__ void __launch_bounds__(kRealWarps * 32) real_pair_kernel(RealArgs A) 
     if (lane == 0) grp = atomicAdd(A.next, 1);
     grp = __shfl_sync(0xffffffffu, grp, 0);
     if (grp >= A.ngroups) break;
-    real_group(A, grp, cand_all[warp], candz_all[warp], tab);
+    real_group(A, grp, cand_all[warp], candz_all[warp], cart_all[warp], tab);
   }
 }
 
@@ -401,6 +428,7 @@ int launch_real_space(const Geom &coarse, const double L[6], int n, const double
     A.cy = (float)(L[5] / coarse.K2);
     A.eta = eta;
     A.rc2 = rcut * rcut;
+    A.rc2l = A.rc2 * 1.0001f;
     A.tab_scale = (float)(kRealTab / xmax);
     A.ngroups = ngroups;
     A.next = next;
