@@ -23,34 +23,35 @@
 // wrap onto itself).  A warp whose points span several rows takes the rows
 // one at a time with the other lanes masked.
 //
-// The candidates are concatenated into one stream and staged 32 at a time in
+// The candidates are concatenated into one stream and staged 64 at a time in
 // shared memory (x, y in cell units relative to the warp's row, the z
 // fraction and charge as a float4; the z cell relative to the warp's lowest z
 // cell as a separate exact integer; the Cartesian position relative to the
-// warp's first cell), read by broadcast: a reject pass over the 32 computes
+// warp's first cell), read by broadcast: a reject pass over the 64 computes
 // every lane's distance (Cartesian, against a cutoff widened by 1e-4 of rc^2
 // to cover its rounding, when no image reduction is needed) and builds its
-// 32-bit mask of candidates inside, then each lane evaluates its accepted pairs one per round
-// (erfc, exp), so the costly part runs on full lanes instead of on the few
-// lanes a candidate happens to be near.  Every pair is visited from both
-// sides, so each point's gradient has one writer and no atomics are needed.
-// Warps take their 32-point groups from a counter (groups differ in work:
-// one or more rows, longer or shorter z runs), and every group writes its own
-// energy / virial partials, summed in group order afterwards, so the result
-// does not depend on which warp took which group.
+// bit masks of candidates inside, then each lane evaluates its accepted pairs
+// one per round (erfc, exp), so the costly part runs on full lanes instead of
+// on the few lanes a candidate happens to be near.  Every pair is visited
+// from both sides, so each point's gradient has one writer and no atomics are
+// needed.  Warps take their 32-point groups from a counter (groups differ in
+// work: one or more rows, longer or shorter z runs), and every group writes
+// its own energy / virial partials, summed in group order afterwards, so the
+// result does not depend on which warp took which group.
 //
 // erfc(x) = exp(-x^2) erfcx(x): the exponential is the one the gradient needs
 // anyway, and erfcx (smooth, between 1 and about 1/(x sqrt(pi))) is a
 // cubic-Hermite table of kRealTab intervals on [0, min(eta rcut, 10)] built
 // in FP64 per call and read from shared memory.
+//
 // Pair terms are FP32; each pair's energy is added in FP64 (the energy is a
 // sum of terms of both signs that cancels to a small fraction of their
-// magnitudes), gradient and virial terms are summed per 32-candidate chunk in
-// FP32 and added to FP64 accumulators per chunk; energy and virial are
-// reduced per block in FP64, then in a fixed order (deterministic).  Separations are
-// integer cell offsets plus the FP32 in-cell fractions of the sort (about
-// 1e-7 cells).  Pairs at zero separation (a point with itself, or two points
-// at the same position) are skipped.
+// magnitudes); gradient and virial terms are summed per staged batch in FP32
+// and added to FP64 accumulators after each batch; energy and virial are
+// reduced per group in FP64, then over groups in a fixed order
+// (deterministic).  Separations are integer cell offsets plus the FP32
+// in-cell fractions of the sort (about 1e-7 cells).  Pairs at zero separation
+// (a point with itself, or two points at the same position) are skipped.
 #include <algorithm>
 #include <cmath>
 
@@ -62,6 +63,7 @@ namespace spme {
 constexpr int kRealWords = 16;  // per-group partials: e, W[6], q^2, q, pad
 constexpr int kRealWarps = 4;   // warps per block of the pair kernel
 constexpr int kRealBlocksPerSM = 6;
+constexpr int kRealStage = 64;  // candidates staged per round of the walk
 
 // Cubic-Hermite table of erfcx(x) = exp(x^2) erfc(x) on [0, xmax]: interval
 // k holds f(k h + t h) = c.x + t (c.y + t (c.z + t c.w)), t in [0, 1].
@@ -140,20 +142,18 @@ __device__ __forceinline__ float pair_r2(const RealArgs &A, const RealLane &L, f
   return dxv * dxv + dyv * dyv + dzv * dzv;
 }
 
-// One staged chunk of 32 candidates: the reject pass, then the accepted pairs
-// one per round.  `live`: the candidates of the chunk this lane takes (none
-// for a lane outside the current row, none past the stream's end).
+// Reject pass over 32 staged candidates: the bit mask of those inside the
+// cutoff (zero separations are dropped later).
 template <bool WRAP>
-__device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const float4 *__restrict__ cand,
-                                           const float *__restrict__ candz, const float4 *__restrict__ cart,
-                                           const float4 *__restrict__ tab, unsigned live) {
+__device__ __forceinline__ unsigned real_reject(const RealArgs &A, const RealLane &L, const float4 *__restrict__ cand,
+                                                const float *__restrict__ candz, const float4 *__restrict__ cart) {
   unsigned mask = 0;
   if (WRAP) {
 #pragma unroll 8
     for (int k = 0; k < 32; k++) {
       float dxv, dyv, dzv;
       const float r2 = pair_r2<WRAP>(A, L, cand[k], candz[k], dxv, dyv, dzv);
-      mask |= (r2 < A.rc2) ? (1u << k) : 0u;  // zero separations are dropped below
+      mask |= (r2 < A.rc2) ? (1u << k) : 0u;
     }
   } else {
     // no image reduction: a plain Cartesian distance against the widened
@@ -166,18 +166,38 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
       mask |= (r2 < A.rc2l) ? (1u << k) : 0u;
     }
   }
-  mask &= live;
+  return mask;
+}
+
+// One staged batch of kRealStage candidates: the reject passes, then the
+// accepted pairs one per round (rounds: the most any lane accepted in the
+// batch).  live0 / live1: the candidates of each half this lane takes (none
+// for a lane outside the current row, none past the stream's end); two: the
+// second half holds candidates (warp-uniform).
+template <bool WRAP>
+__device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const float4 *__restrict__ cand,
+                                           const float *__restrict__ candz, const float4 *__restrict__ cart,
+                                           const float4 *__restrict__ tab, unsigned live0, unsigned live1,
+                                           bool two) {
+  unsigned m0 = real_reject<WRAP>(A, L, cand, candz, cart) & live0;
+  unsigned m1 = two ? real_reject<WRAP>(A, L, cand + 32, candz + 32, cart + 32) & live1 : 0u;
   const float two_eta_sqrtpi = 1.1283791670955126f * A.eta;  // 2 eta / sqrt(pi)
   const float eta2 = A.eta * A.eta;
-  while (mask) {
-    const int k = __ffs(mask) - 1;
-    mask &= mask - 1;
+  while (m0 | m1) {
+    int k;
+    if (m0) {
+      k = __ffs(m0) - 1;
+      m0 &= m0 - 1;
+    } else {
+      k = 31 + __ffs(m1);
+      m1 &= m1 - 1;
+    }
     const float4 c = cand[k];
     float dxv, dyv, dzv;
     const float r2 = pair_r2<WRAP>(A, L, c, candz[k], dxv, dyv, dzv);
     if (!(r2 < A.rc2) || r2 == 0.f) continue;  // outside the cutoff; the point itself (or a coincident one)
     const float ir = rsqrtf(r2);
-    const float ex = expf(-eta2 * r2);  // exp(-x^2), x = eta r
+    const float ex = __expf(-eta2 * r2);  // exp(-x^2), x = eta r (error grows with x^2, where the term is small)
     const float u = A.eta * (r2 * ir) * A.tab_scale;
     const int ti = min((int)u, kRealTab - 1);
     const float tt = fminf(u - (float)ti, 1.f);
@@ -301,8 +321,10 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
     }
     const int total = __shfl_sync(0xffffffffu, pre, 31);
     pre -= l1 + l2;
-    for (int v0 = 0; v0 < total; v0 += 32) {
-      const int v = v0 + lane;
+    for (int v0 = 0; v0 < total; v0 += kRealStage) {
+#pragma unroll
+     for (int b = 0; b < kRealStage / 32; b++) {
+      const int v = v0 + 32 * b + lane;
       float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);  // past the end: masked out below
       float cvz = 0.f;
       float4 cvp = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -328,17 +350,19 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
         const float zc = cvz + rj.z;
         cvp = make_float4(cv.x * A.ax + cv.y * A.bx + zc * A.cx, cv.y * A.by + zc * A.cy, zc * A.cz, 0.f);
       }
+      cand[32 * b + lane] = cv;
+      candz[32 * b + lane] = cvz;
+      cart[32 * b + lane] = cvp;
+     }
       __syncwarp();
-      cand[lane] = cv;
-      candz[lane] = cvz;
-      cart[lane] = cvp;
-      __syncwarp();
-      const int cnt = total - v0;
-      const unsigned live = act ? (cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u) : 0u;
+      const int cnt = total - v0;  // candidates left in the stream, > 0
+      const unsigned live0 = act ? (cnt >= 32 ? 0xffffffffu : (1u << cnt) - 1u) : 0u;
+      const unsigned live1 = (act && cnt > 32) ? (cnt >= 64 ? 0xffffffffu : (1u << (cnt - 32)) - 1u) : 0u;
       if (wrap)
-        real_chunk<true>(A, L, cand, candz, cart, tab, live);
+        real_chunk<true>(A, L, cand, candz, cart, tab, live0, live1, cnt > 32);
       else
-        real_chunk<false>(A, L, cand, candz, cart, tab, live);
+        real_chunk<false>(A, L, cand, candz, cart, tab, live0, live1, cnt > 32);
+      __syncwarp();  // every lane has read the batch before the next one is staged
     }
   }
   double acc[9];
@@ -366,9 +390,9 @@ __device__ __forceinline__ void real_group(const RealArgs &A, int grp, float4 *c
 }
 
 __global__ void __launch_bounds__(kRealWarps * 32, kRealBlocksPerSM) real_pair_kernel(RealArgs A) {
-  __shared__ float4 cand_all[kRealWarps][32];
-  __shared__ float candz_all[kRealWarps][32];
-  __shared__ float4 cart_all[kRealWarps][32];
+  __shared__ float4 cand_all[kRealWarps][kRealStage];
+  __shared__ float candz_all[kRealWarps][kRealStage];
+  __shared__ float4 cart_all[kRealWarps][kRealStage];
   __shared__ float4 tab[kRealTab];
   for (int k = threadIdx.x; k < kRealTab; k += blockDim.x) tab[k] = A.tab[k];
   __syncthreads();
