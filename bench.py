@@ -179,6 +179,11 @@ STAGE_KERNELS = {
 SINGLE_KERNEL_STAGES = ("spread", "convolution", "gather")
 
 
+def volume(L):
+    """Cell volume from the 6-vector [ax, by, cz, bx, cx, cy] (lower-triangular box)."""
+    return float(L[0] * L[1] * L[2])
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -425,7 +430,11 @@ def run_b200(args, rank, world, local_rank):
         },
         "gpu_launches": int(launches),
         "real_space": {"ms": real_ms, "rcut_nm": 1.0, "eta": c.beta,
-                       "note": "erfc pair sum + self/background terms (sfac_real_space_device); not in the metric"},
+                       # ordered pairs within the cutoff from the mean density
+                       # (each pair is evaluated from both sides)
+                       "pairs_per_s": n * (n / volume(c.L)) * (4.0 / 3.0) * math.pi * 1.0 ** 3 / (real_ms / 1e3),
+                       "note": "erfc pair sum + self/background terms (sfac_real_space_device), cell sort "
+                               "included; not in the metric"},
         "energy": float(ev_host[0]),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
