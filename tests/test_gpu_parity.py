@@ -165,10 +165,13 @@ def _sort_inputs():
                           rng.uniform(0, 2, size=(300, 3)), 1.26 + rng.uniform(0, 0.1, size=(300, 3))])
     out.append(("large_cells", Lc, K, rng.permutation(big)))
     out.append(("one_cell", Lc, K, np.full((4097, 3), 0.7)))
+    # a grid above the single-launch sort's cell limit: the multi-kernel sort
+    out.append(("grid168", np.array([6.0, 5.5, 6.2, 0.8, -0.5, 0.4]), (168, 168, 168),
+                rng.uniform(-2, 8, size=(20000, 3))))
     return out
 
 
-@pytest.mark.parametrize("case", range(7))
+@pytest.mark.parametrize("case", range(8))
 def test_cell_sort_bit_exact(case):
     name, L, K, x = _sort_inputs()[case]
     ew = E()
