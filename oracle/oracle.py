@@ -300,6 +300,28 @@ def real_space(L, x, q, eta, rcut):
     return e, e_self, e_net, vir, dx
 
 
+def real_space_scale(L, x, q, eta, rcut):
+    """Sum of |pair energies| of real_space's E_real, 1/2 sum |q_i q_j| erfc(eta r)/r
+    over the same pairs: the magnitude against which the rounding of a sum of
+    terms of both signs is measured."""
+    from scipy.special import erfc
+
+    Lm = LofS(L)
+    s = np.asarray(x, dtype=np.float64) @ np.linalg.inv(Lm)
+    q = np.asarray(q, dtype=np.float64)
+    n = len(q)
+    tot = 0.0
+    for i in range(n):
+        ds = s - s[i]
+        ds -= np.rint(ds)
+        d = ds @ Lm
+        r2 = np.einsum("ij,ij->i", d, d)
+        mask = (r2 < rcut * rcut) & (np.arange(n) != i)
+        r = np.sqrt(r2[mask])
+        tot += 0.5 * np.sum(np.abs(q[i] * q[mask]) * erfc(eta * r) / r)
+    return tot
+
+
 def sk_radial(L, K, acc, nbins, kmax):
     """FP64 restatement of the radial binning of a sum of |S|^2 over the
     stored half-space modes (the reference's plot.py:9-32, on the general
