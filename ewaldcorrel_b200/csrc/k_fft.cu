@@ -610,6 +610,59 @@ __global__ void __launch_bounds__(512) fft_y2_kernel(int n, int n1, int n2, cons
   }
 }
 
+// Copies the contiguous block src[0 .. valid) (elements of T in rows of
+// `width`) into sh[r * pitch + c] for the first `total` elements, zero past
+// `valid`.  16-byte loads, four per thread issued before any of them is
+// stored, so that a small CTA keeps many loads in flight (a row-by-row loop
+// whose stores wait on each load leaves one in flight per thread); the row
+// and column of each element are advanced incrementally.  src must be
+// 16-byte aligned.
+template <typename T>
+__device__ __forceinline__ void stage_rows(const T *__restrict__ src, int valid, int total, int width, int pitch,
+                                           T *sh) {
+  constexpr int PER = 16 / sizeof(T);
+  const int nv = (total + PER - 1) / PER;
+  const int step = PER * blockDim.x;  // elements per pass of the CTA
+  const int sr = step / width, sc = step - sr * width;
+  int r = (PER * threadIdx.x) / width, c = PER * threadIdx.x - r * width;
+  for (int i = threadIdx.x; i < nv; i += 4 * blockDim.x) {
+    float4 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int iu = i + u * blockDim.x, f = iu * PER;
+      if (iu < nv && f + PER <= valid) {
+        v[u] = __ldg(reinterpret_cast<const float4 *>(src) + iu);
+      } else {
+        T *e = reinterpret_cast<T *>(&v[u]);
+#pragma unroll
+        for (int k = 0; k < PER; k++) e[k] = (iu < nv && f + k < valid) ? src[f + k] : T{};
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int iu = i + u * blockDim.x;
+      if (iu < nv) {
+        const T *e = reinterpret_cast<const T *>(&v[u]);
+        int rr = r, cc = c;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+          if (iu * PER + k < total) sh[rr * pitch + cc] = e[k];
+          if (++cc == width) {
+            cc = 0;
+            rr++;
+          }
+        }
+      }
+      r += sr;
+      c += sc;
+      if (c >= width) {
+        c -= width;
+        r++;
+      }
+    }
+  }
+}
+
 // z pass, real to half-complex: 2B consecutive real rows of length n per
 // CTA (row pair b forms the complex line row[2b] + i row[2b+1]); the rows
 // are read and the ldim = n/2 + 1 outputs written as contiguous blocks.
@@ -626,8 +679,12 @@ __global__ void __launch_bounds__(512) fft_zr2c2_kernel(int n, int n1, int n2, c
   const int nr = (int)min((long)(2 * B), nrows - row0);
   const float *src = rin + row0 * n;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
-    for (int j = lane; j < n; j += 32) rows[rr * RP + j] = (rr < nr) ? src[(long)rr * n + j] : 0.f;
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    stage_rows<float>(src, nr * n, 2 * B * n, n, RP, rows);
+  } else {
+    for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
+      for (int j = lane; j < n; j += 32) rows[rr * RP + j] = (rr < nr) ? src[(long)rr * n + j] : 0.f;
+  }
   __syncthreads();
   const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
   if (t < n2) {
@@ -685,8 +742,13 @@ __global__ void __launch_bounds__(512) fft_zc2r2_kernel(int n, int n1, int n2, c
   const int nr = (int)min((long)(2 * B), nrows - row0);
   const float2 *src = cin + row0 * ldim;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
-    for (int k = lane; k < ldim; k += 32) H[rr * HP + k] = (rr < nr) ? src[(long)rr * ldim + k] : make_float2(0.f, 0.f);
+  if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+    stage_rows<float2>(src, nr * ldim, 2 * B * ldim, ldim, HP, H);
+  } else {
+    for (int rr = threadIdx.x >> 5; rr < 2 * B; rr += nw)
+      for (int k = lane; k < ldim; k += 32)
+        H[rr * HP + k] = (rr < nr) ? src[(long)rr * ldim + k] : make_float2(0.f, 0.f);
+  }
   __syncthreads();
   const int b = threadIdx.x & (B - 1), t = threadIdx.x >> lgB;
   if (t < n2) {
