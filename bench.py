@@ -55,8 +55,8 @@ def _env_int(name, default):
 class ClockSampler:
     """SM clocks and throttle reasons sampled while the GPU works: an NVML
     polling thread (every 2 ms, so that a timed region of a few milliseconds
-    still gets samples), with `nvidia-smi -lms 100` written beside it to
-    gpurun_out/clocks_rank<i>.csv as a second record."""
+    still gets samples), with `nvidia-smi -lms 100` written beside it to a
+    per-rank CSV in the run's output folder as a second record."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"

@@ -1,6 +1,6 @@
 """Helpers shared by the GPU parity tests: run one full solve through the
 B200 library's C ABI (via the ewald.py-compatible wrapper) and through the
-FP64 CPU oracle, and compare with the north-star error measures."""
+FP64 CPU oracle, and compare by relative RMS force error and relative energy error."""
 from __future__ import annotations
 
 import numpy as np
