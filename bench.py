@@ -161,10 +161,10 @@ def algorithmic_bytes(n, K):
 # profiles/dram_per_kernel_water_triclinic.md).  Writes that stay in the
 # 126 MB L2 past the kernel's end are not counted by the capture.
 NCU_TRAFFIC = {
-    "water": {"cell_sort": 24.19e6, "spread": 5.52e6, "fft_forward": 7.30e6, "convolution": 29.00e6,
-              "fft_inverse": 7.41e6, "gather": 7.10e6},
-    "triclinic": {"cell_sort": 438.56e6, "spread": 124.86e6, "fft_forward": 164.31e6, "convolution": 163.80e6,
-                  "fft_inverse": 166.09e6, "gather": 158.09e6},
+    "water": {"cell_sort": 24.20e6, "spread": 5.52e6, "fft_forward": 7.30e6, "convolution": 29.00e6,
+              "fft_inverse": 7.41e6, "gather": 6.70e6},
+    "triclinic": {"cell_sort": 438.63e6, "spread": 124.81e6, "fft_forward": 163.58e6, "convolution": 163.50e6,
+                  "fft_inverse": 165.67e6, "gather": 158.32e6},
 }
 # Kernels of each stage (the roofline is reported for the longest stage that
 # is a single kernel launch).
