@@ -157,13 +157,19 @@ __device__ __forceinline__ unsigned real_reject(const RealArgs &A, const RealLan
     }
   } else {
     // no image reduction: a plain Cartesian distance against the widened
-    // cutoff; the accepted pairs are tested again from the exact separation
-#pragma unroll 8
-    for (int k = 0; k < 32; k++) {
-      const float4 p = cart[k];
-      const float ddx = p.x - L.px, ddy = p.y - L.py, ddz = p.z - L.pz;
-      const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
-      mask |= (r2 < A.rc2l) ? (1u << k) : 0u;
+    // cutoff; the accepted pairs are tested again from the exact separation.
+    // Eight candidates per byte of the mask, each with a constant bit.
+#pragma unroll 1
+    for (int k0 = 0; k0 < 32; k0 += 8) {
+      unsigned byte = 0;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const float4 p = cart[k0 + c];
+        const float ddx = p.x - L.px, ddy = p.y - L.py, ddz = p.z - L.pz;
+        const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        byte |= (r2 < A.rc2l) ? (1u << c) : 0u;
+      }
+      mask |= byte << k0;
     }
   }
   return mask;
@@ -207,15 +213,16 @@ __device__ __forceinline__ void real_chunk(const RealArgs &A, RealLane &L, const
     const float qq = L.q * c.w;
     const float t = -qq * (two_eta_sqrtpi * ex + phi) * ir * ir;  // q q phi'(r) / r
     L.E += (double)(qq * phi);
-    L.g0 -= t * dxv;
-    L.g1 -= t * dyv;
-    L.g2 -= t * dzv;
-    L.w[0] += t * dxv * dxv;
-    L.w[1] += t * dyv * dyv;
-    L.w[2] += t * dzv * dzv;
-    L.w[3] += t * dyv * dxv;
-    L.w[4] += t * dzv * dxv;
-    L.w[5] += t * dzv * dyv;
+    const float tx = t * dxv, ty = t * dyv, tz = t * dzv;
+    L.g0 -= tx;
+    L.g1 -= ty;
+    L.g2 -= tz;
+    L.w[0] = fmaf(tx, dxv, L.w[0]);
+    L.w[1] = fmaf(ty, dyv, L.w[1]);
+    L.w[2] = fmaf(tz, dzv, L.w[2]);
+    L.w[3] = fmaf(ty, dxv, L.w[3]);
+    L.w[4] = fmaf(tz, dxv, L.w[4]);
+    L.w[5] = fmaf(tz, dyv, L.w[5]);
   }
   // chunk partials into the FP64 totals (each pair is visited from both
   // sides: half of the virial; the energy is halved at the end)
