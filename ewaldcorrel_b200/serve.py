@@ -308,3 +308,25 @@ def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, d
         "autotuned_shapes": len(tunes),
         "mean_atoms": float(np.mean([r.n for r in reqs])),
     }
+
+
+def main(argv=None):
+    """`python -m ewaldcorrel_b200.serve [--count N] [--plain N] [--load F]`:
+    runs stream_benchmark on GPU 0 and prints its results as one JSON line."""
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--count", type=int, default=3000)
+    ap.add_argument("--plain", type=int, default=1000)
+    ap.add_argument("--load", type=float, default=0.8)
+    ap.add_argument("--max-inflight", type=int, default=48)
+    args = ap.parse_args(argv)
+    t0 = time.perf_counter()
+    res = stream_benchmark(count=args.count, plain_count=args.plain, load=args.load, max_inflight=args.max_inflight)
+    res["wall_s"] = time.perf_counter() - t0
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
