@@ -249,6 +249,24 @@ def cpu_baseline(c, budget_s=20.0, max_solves=10):
 E2E_MIN_STEPS = 100
 
 
+def max_over_ranks(ms, dist, device):
+    """The largest of every rank's `ms` (each rank's own device-timed total):
+    the whole job ends when its slowest rank does.  dist: torch.distributed
+    with an initialised process group, or None for one rank."""
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rate_over_ranks(units, ms_max):
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time (ms)."""
+    return units / (ms_max / 1e3)
+
+
 def bind_gpu_local_cpus(local_rank):
     """Binds this process to the CPUs that NVML reports as local to its GPU
     (the NUMA node of the GPU's PCIe root), so that the pinned host buffers
@@ -344,11 +362,8 @@ def run_b200(args, rank, world, local_rank):
     launches = solver.launches() - l0
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = sum(step_ms)
-    tmax = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    total_ms_max = float(tmax.item())
-    value = world * K / (total_ms_max / 1e3)
+    total_ms_max = max_over_ranks(total_ms, dist, dev)
+    value = rate_over_ranks(world * K, total_ms_max)
     srt = sorted(step_ms)
     p50 = srt[len(srt) // 2]
     p99 = srt[min(len(srt) - 1, int(math.ceil(0.99 * len(srt))) - 1)]
@@ -412,10 +427,7 @@ def run_b200(args, rank, world, local_rank):
     clocks = clk.summary()
     clocks["window"] = "warm-up, timed steps, per-stage timing and the e2e run"
     clocks["timed_steps"] = clk.summary(c0, c1)
-    e2e_t = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * KE / (float(e2e_t.item()) / 1e3)
+    e2e_value = rate_over_ranks(world * KE, max_over_ranks(sum(e2e_ms), dist, dev))
 
     line = {
         "metric": METRIC,
