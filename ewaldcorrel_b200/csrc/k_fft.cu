@@ -1018,8 +1018,11 @@ static int x_lines_per_cta(const FftPlan3 &F, int n, long nlines) {
 }
 
 // Two-level x pass: lines per CTA B = 2^lgB (8..32) with B*max(n1, n2)
-// threads (<= 512), halved while fewer than two CTAs per SM would run;
-// x_lines overrides B.  Returns false when K0 has no n1 * n2 split.
+// threads (<= 512): grown to CTAs of at least 8 warps (each CTA pays for its
+// twiddles and setup once), halved only while the SMs would not all get one
+// (up to 1/16 of them may idle: 147 CTAs of 32 lines beat 294 of 16 and 588
+// of 8 for a 96^3 grid, 98 vs 100 vs 102 us per solve); x_lines overrides B.
+// Returns false when K0 has no n1 * n2 split.
 static bool x2_shape(const FftPlan3 &F, int n, long nlines, int &n1, int &n2, int &lgB, int &threads) {
   if (!rdft::split_line(n, n1, n2)) return false;
   const int m = n1 > n2 ? n1 : n2;
@@ -1029,8 +1032,8 @@ static bool x2_shape(const FftPlan3 &F, int n, long nlines, int &n1, int &n2, in
     while (B < F.x_lines && B < 32) B <<= 1;
   } else {
     B = 8;
-    while (B < 32 && B * m < 128) B <<= 1;
-    while (B > 8 && (nlines + B - 1) / B < 2 * 148) B >>= 1;
+    while (B < 32 && B * m < 256) B <<= 1;
+    while (B > 8 && (nlines + B - 1) / B < 148 - 148 / 16) B >>= 1;
   }
   while (B > 8 && B * m > 512) B >>= 1;
   if (B * m > 512) return false;
