@@ -2,11 +2,13 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Workload: the water box (98,304 atoms = 32,768 rigid 3-site molecules in a
-10 nm cube, 96^3 grid, B-spline order 4, Ewald beta 3.12 nm^-1), seeded
-synthetic data.  One step = one full reciprocal solve: cell sort, spread,
-forward FFT, convolution with energy and virial, inverse FFT, and the gather
-of forces (dE/dx) and potentials at every atom.
+Workload (default ``--workload triclinic``): the largest single-GPU system,
+1,048,576 charges N(0, 0.5^2) in a triclinic cell (a=b=c=20 nm, gamma=60
+deg), 256^3 grid, B-spline order 6, Ewald beta 3.5 nm^-1, seeded synthetic
+data; ``--workload water`` takes the 98,304-atom water box (96^3, order 4)
+instead.  One step = one full reciprocal solve: cell sort, spread, forward
+FFT, convolution with energy and virial, inverse FFT, and the gather of
+forces (dE/dx) and potentials at every atom.
 
 Metric: solves/s (whole job; replicas on N GPUs -- the path does not shard).
 ``value`` is timed with CUDA events on the launching stream with inputs
@@ -40,8 +42,23 @@ WORKLOADS = {
                   "B-spline order 6, Ewald beta 3.5 nm^-1",
                   "SPME solves/s (1,048,576 charges, 256^3, order 6, triclinic)"),
 }
-WORKLOAD, METRIC = WORKLOADS["water"]
+DEFAULT_WORKLOAD = "triclinic"
 L2_FLUSH_BYTES = 256 << 20
+# The reference arm runs whole solves on the host's cores; at the 1M-atom size
+# one solve takes seconds, so its timed steps stop once this many seconds of
+# solves have run (each step stays one whole solve; the line says how many).
+REFERENCE_BUDGET_S = float(os.environ.get("SPME_REFERENCE_BUDGET_S", "100"))
+
+
+def load_workload(name):
+    """The seeded system of a workload name (see WORKLOADS)."""
+    from ewaldcorrel_b200 import configs
+
+    return configs.cfg2_water() if name == "water" else configs.cfg3_triclinic()
+
+
+def workload_seed(name):
+    return 2 if name == "water" else 3
 
 
 def _env_int(name, default):
@@ -56,7 +73,8 @@ class ClockSampler:
     """SM clocks and throttle reasons sampled while the GPU works: an NVML
     polling thread (every 2 ms, so that a timed region of a few milliseconds
     still gets samples), with `nvidia-smi -lms 100` written beside it to a
-    per-rank CSV in the run's output folder as a second record."""
+    per-rank CSV as a second record when SPME_BENCH_CLOCKS_DIR names a
+    folder for it."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -67,7 +85,8 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        d = os.environ.get("SPME_BENCH_CLOCKS_DIR")
+        self.path = os.path.join(d, f"clocks_rank{index}.csv") if d else None
         self.samples = []  # (sm_mhz, reasons bitmask)
         self.smax = None
         self._stop = None
@@ -95,6 +114,8 @@ class ClockSampler:
         self._thread = threading.Thread(target=self._poll, daemon=True)
         self._thread.start()
         try:
+            if self.path is None:
+                raise OSError("no clocks CSV folder")
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -224,7 +245,7 @@ def cpu_solve(s, c):
     return e, vir, dx, phi
 
 
-def cpu_baseline(c, budget_s=20.0, max_solves=10):
+def cpu_baseline(c, label, budget_s=20.0, max_solves=10):
     cls, kind, desc = _load_reference_solver()
     s = cpu_setup(cls, c)
     t0 = time.perf_counter()
@@ -240,7 +261,7 @@ def cpu_baseline(c, budget_s=20.0, max_solves=10):
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {
         "value": 1.0 / per, "unit": "solves/s", "cores": cores, "kind": kind,
-        "sample": f"{len(times)} full water-box solves (sfac+de1+de2+potl, setup excluded), median {per * 1e3:.1f} ms; {desc}",
+        "sample": f"{len(times)} full {label} solves (sfac+de1+de2+potl, setup excluded), median {per * 1e3:.1f} ms; {desc}",
     }, res
 
 
@@ -300,7 +321,6 @@ def bind_gpu_local_cpus(local_rank):
 def run_b200(args, rank, world, local_rank):
     import torch
 
-    from ewaldcorrel_b200 import configs
     from ewaldcorrel_b200 import ewald as ew
     from ewaldcorrel_b200.device import STAGES, SpmeSolver
 
@@ -315,7 +335,7 @@ def run_b200(args, rank, world, local_rank):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    c = configs.cfg2_water() if args.workload == "water" else configs.cfg3_triclinic()
+    c = load_workload(args.workload)
     WORKLOAD, METRIC = WORKLOADS[args.workload]
     n = c.n
     stream = torch.cuda.Stream(dev)
@@ -441,7 +461,7 @@ def run_b200(args, rank, world, local_rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32 (grids, FFT, spline weights); f64 (positions, cell keys, moduli, influence function, energy/virial reductions)",
-        "data": f"synthetic (seeded numpy rng({2 if args.workload == 'water' else 3}); no dataset)",
+        "data": f"synthetic (seeded numpy rng({workload_seed(args.workload)}); no dataset)",
         "config": {
             "workload": WORKLOAD,
             "atoms": n,
@@ -493,7 +513,7 @@ def run_b200(args, rank, world, local_rank):
     if prev_cpus is not None:
         os.sched_setaffinity(0, prev_cpus)  # the CPU baseline uses every host core
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb, (e_ref, vir_ref, dx_ref, phi_ref) = cpu_baseline(c)
+        cb, (e_ref, vir_ref, dx_ref, phi_ref) = cpu_baseline(c, args.workload)
         line["cpu_baseline"] = cb
         dxg = dx.cpu().numpy()
         phig = phi.cpu().numpy()
@@ -513,27 +533,42 @@ def run_b200(args, rank, world, local_rank):
 
 # ------------------------------------------------------ reference arm --
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the solve (oracle/_ref: its
+    sfac.cpp compiled unmodified; the oracle's C restatement where the
+    reference was not built) on this host's cores, on the same workload,
+    metric and unit as the GPU arm.  Rank 0 alone runs and prints the line.
+
+    Each step is one whole solve (sfac + de1 + de2 + potl).  At the 1M-atom
+    size a solve takes seconds, so the run is bounded: warm-up stops after
+    the first solve once W solves or a tenth of REFERENCE_BUDGET_S have run,
+    and the timed steps stop once K steps or REFERENCE_BUDGET_S seconds have
+    run (at least one step); `steps` is the number timed, `steps_requested`
+    the K asked for."""
     if rank != 0:
         return
-    from ewaldcorrel_b200 import configs
-
     try:
         cls, kind, desc = _load_reference_solver()
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"CPU reference not built: {e}"}))
         return
-    c = configs.cfg2_water()
+    WORKLOAD, METRIC = WORKLOADS[args.workload]
+    c = load_workload(args.workload)
     s = cpu_setup(cls, c)
-    for _ in range(max(0, args.warmup)):
+    warm, t_warm = 0, 0.0
+    while warm < max(0, args.warmup) and (warm == 0 or t_warm < 0.1 * REFERENCE_BUDGET_S):
+        a = time.perf_counter()
         cpu_solve(s, c)
+        t_warm += time.perf_counter() - a
+        warm += 1
     times = []
-    for _ in range(args.steps):
+    while len(times) < max(1, args.steps) and (not times or sum(times) < REFERENCE_BUDGET_S):
         a = time.perf_counter()
         cpu_solve(s, c)
         times.append(time.perf_counter() - a)
     s.close()
+    steps = len(times)
     total = sum(times)
-    value = args.steps / total
+    value = steps / total
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     srt = sorted(times)
     line = {
@@ -542,19 +577,22 @@ def run_reference(args, rank, world):
         "value": value,
         "unit": "solves/s",
         "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": total / args.steps * 1e3,
+        "steps": steps,
+        "steps_requested": args.steps,
+        "warmup": warm,
+        "warmup_requested": args.warmup,
+        "ms_per_step": total / steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded numpy rng(2); no dataset)",
+        "data": f"synthetic (seeded numpy rng({workload_seed(args.workload)}); no dataset)",
         "config": {"workload": WORKLOAD, "atoms": c.n, "grid": list(c.K), "order": c.order, "beta": c.beta,
                    "max_m": c.max_m, "parallelism": "CPU, OpenMP threads"},
         "latency_ms": {"p50": srt[len(srt) // 2] * 1e3, "p99": srt[-1] * 1e3},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind,
-                         "sample": f"{args.steps} full water-box solves (sfac+de1+de2+potl, setup excluded); {desc}"},
+                         "sample": (f"{steps} full {args.workload} solves (sfac+de1+de2+potl, setup excluded; "
+                                    f"run bounded at {REFERENCE_BUDGET_S:.0f} s); {desc}")},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -572,7 +610,7 @@ def run_profile(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    c = configs.cfg2_water() if args.workload == "water" else configs.cfg3_triclinic()
+    c = load_workload(args.workload)
     stream = torch.cuda.Stream(dev)
     solver = SpmeSolver(c.L, c.K, c.order, c.beta, c.max_m, device=0, stream=stream)
     solver.lib.sfac_set_graphs(solver.handle, 0)
@@ -601,7 +639,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="run this many plain solves for a profiler capture and exit (no timing line)")
     args = ap.parse_args(argv)

@@ -509,9 +509,14 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocBytes];
 
 // Device address of g_sort_scratch, looked up once per device (the host-side
 // symbol is only a stand-in: a kernel must be given this address instead).
+// The cached address belongs to the device's primary context: it does not
+// survive cudaDeviceReset, after which this entry point must not be called.
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Writes the box constants (a kernel argument) to device memory.
+__global__ void store_cell_kernel(CellConst c, CellConst *dst) { *dst = c; }
 
 unsigned char *noalloc_scratch() {
   int dev = 0;
@@ -554,12 +559,11 @@ extern "C" int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, 
   if (!base) return 2;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  // Box constants with the reference's expressions (sfac.hpp:45-51), copied
-  // into the scratch array (the copy of this pageable source completes
-  // before cudaMemcpyAsync returns).
-  const CellConst cell = make_cell(L);
+  // Box constants with the reference's expressions (sfac.hpp:45-51), written
+  // into the scratch array by a one-thread kernel that takes them by value:
+  // no host address is handed to the stream.
   CellConst *dcell = reinterpret_cast<CellConst *>(base + kNaCell);
-  if (cudaMemcpyAsync(dcell, &cell, sizeof(cell), cudaMemcpyHostToDevice, st) != cudaSuccess) return 2;
+  store_cell_kernel<<<1, 1, 0, st>>>(make_cell(L), dcell);
   Geom g{};
   g.K0 = K[0];
   g.K1 = K[1];

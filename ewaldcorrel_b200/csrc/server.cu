@@ -230,7 +230,7 @@ int spme_server_submit(void *p, long long id, int n, const int K[3], int order, 
   return 0;
 }
 
-int spme_server_poll(void *p, long long *ids, int max_ids) {
+int spme_server_poll(void *p, long long *ids, int *status, int max_ids) {
   Server *sv = static_cast<Server *>(p);
   if (!sv || !ids) return 0;
   int c = 0;
@@ -239,13 +239,17 @@ int spme_server_poll(void *p, long long *ids, int max_ids) {
     if (!s->busy) continue;
     const cudaError_t e = cudaEventQuery(s->done);
     if (e == cudaErrorNotReady) continue;
-    if (e != cudaSuccess) {
+    int st = 0;
+    if (e != cudaSuccess) {  // the request's work failed: its outputs are not valid
       cudaGetLastError();
       sv->errors++;
+      st = 2;
+    } else {
+      sv->solves++;
     }
     s->busy = false;
     sv->inflight--;
-    sv->solves++;
+    if (status) status[c] = st;
     ids[c++] = s->id;
   }
   return c;

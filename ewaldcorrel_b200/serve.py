@@ -41,7 +41,7 @@ def _lib():
         lib.spme_server_submit.argtypes = [c_void_p, c_longlong, c_int, _int3, c_int, c_double, c_double, _dbl6,
                                            c_void_p, c_void_p, c_void_p]
         lib.spme_server_submit.restype = c_int
-        lib.spme_server_poll.argtypes = [c_void_p, POINTER(c_longlong), c_int]
+        lib.spme_server_poll.argtypes = [c_void_p, POINTER(c_longlong), POINTER(c_int), c_int]
         lib.spme_server_poll.restype = c_int
         lib.spme_server_tune.argtypes = [c_void_p, _int3, c_int, c_int]
         lib.spme_server_tune.restype = c_int
@@ -79,6 +79,7 @@ class SpmeServer:
         if not self.h:
             raise RuntimeError("spme_server_create failed (no CUDA device?)")
         self._ids = (c_longlong * 1024)()
+        self._status = (c_int * 1024)()
 
     def close(self):
         if self.h:
@@ -98,8 +99,10 @@ class SpmeServer:
                                            xbuf.ctypes.data, req.q.ctypes.data, out.ctypes.data)
 
     def poll(self):
-        k = self.lib.spme_server_poll(self.h, self._ids, 1024)
-        return [self._ids[i] for i in range(k)]
+        """Completed requests as (id, status): status 0 means the output
+        buffer holds the results, 2 that the request's GPU work failed."""
+        k = self.lib.spme_server_poll(self.h, self._ids, self._status, 1024)
+        return [(self._ids[i], self._status[i]) for i in range(k)]
 
     def tune(self, K, order, x_lines):
         self.lib.spme_server_tune(self.h, np.asarray(K, np.int32), int(order), int(x_lines))
@@ -151,8 +154,10 @@ def run_stream(server: SpmeServer, requests, arrivals=None, make_x=None, max_inf
         ids = server.poll()
         if ids:
             tdone = time.perf_counter() - t0
-            for rid in ids:
+            for rid, st in ids:
                 i, xb, ob = inflight.pop(rid)
+                if st != 0:
+                    raise RuntimeError(f"request {rid} failed on the GPU (status {st})")
                 lat[i] = tdone - arr[i]
                 if keep is not None and rid in keep:
                     r = requests[i]

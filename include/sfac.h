@@ -200,7 +200,9 @@ int sfac_solve_device_timed(void *sfac, int n, const double *x, const double *w,
  * Every call on a device shares that array and leaves its contents behind,
  * so calls whose GPU work overlaps (other streams or threads) race.  The
  * first call on a device looks up the array's device address with that
- * device current; make it before any stream capture begins.
+ * device current; make it before any stream capture begins.  That address
+ * is kept for the life of the process: do not call this after
+ * cudaDeviceReset on that device.
  * Returns 0, 1 (bad arguments or n too large), 2 (CUDA error). */
 int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, const double *x, int *keys, int *perm,
                            void *stream);
@@ -239,7 +241,10 @@ void *spme_server_create(int device, double budget_bytes, int max_inflight, int 
 void spme_server_destroy(void *server);
 int spme_server_submit(void *server, long long id, int n, const int K[3], int order, double beta, double max_m,
                        const double L[6], const double *x, const double *q, double *out);
-int spme_server_poll(void *server, long long *ids, int max_ids);
+/* Completed requests: up to max_ids ids, each with its status (0: out holds
+ * the results; 2: the request's GPU work failed and out is not valid).
+ * status may be NULL.  Returns the number of ids written. */
+int spme_server_poll(void *server, long long *ids, int *status, int max_ids);
 /* Sets x-FFT lines per CTA for slots of grid K and order (autotuner result). */
 int spme_server_tune(void *server, const int K[3], int order, int x_lines);
 /* stats[0..7] = slots, bytes in use, solves, slots created, slots evicted,

@@ -3,7 +3,7 @@ has the reference sources; the fixtures are committed, this script is not
 needed at test time).
 
     make -C oracle all ref
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference PATH]   (default: $EWALDCORREL_REFERENCE, else /root/reference)
 
 Sources of truth:
   * test_log_ref.json  -- the numbers recorded in the reference's own
@@ -110,7 +110,7 @@ def small_systems():
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("EWALDCORREL_REFERENCE", "/root/reference"))
     a = ap.parse_args(argv)
     if not ref_available():
         raise SystemExit("oracle/_ref/libsfac_ref.so is not built: make -C oracle ref")

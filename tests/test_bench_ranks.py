@@ -48,7 +48,7 @@ def test_two_gloo_ranks_agree_on_slowest_time():
 def test_reference_arm_nonzero_rank_prints_nothing():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+                        "--warmup", "1", "--workload", "water"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
 
@@ -56,7 +56,7 @@ def test_reference_arm_nonzero_rank_prints_nothing():
 def test_reference_arm_rank0_reports_world(oracle_built):
     env = dict(os.environ, RANK="0", WORLD_SIZE="2", LOCAL_RANK="0")
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+                        "--warmup", "1", "--workload", "water"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1

@@ -245,6 +245,17 @@ def test_triclinic_order6_against_oracle():
     assert_parity(r, o, c.name)
 
 
+def test_triclinic_1m_full_size_against_oracle():
+    """The 1,048,576-charge triclinic solve (256^3 grid, order 6, beta 3.5)
+    at full size against the FP64 oracle: FP32 in-cell fractions, weights,
+    FFT and gather in a 20 nm box, energy within 1e-6 and forces within
+    1e-5 relative RMS."""
+    c = configs.cfg3_triclinic()
+    r = solve("gpu", c.L, c.K, c.order, c.x, c.q, c.beta, c.max_m)
+    o = solve("oracle", c.L, c.K, c.order, c.x, c.q, c.beta, c.max_m)
+    assert_parity(r, o, c.name)
+
+
 def test_device_ewald_matches_host_table():
     """sfac_set_ewald (device FP64 influence function) == set_A(ewald_f)."""
     ew = E()
