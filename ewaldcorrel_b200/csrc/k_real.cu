@@ -435,7 +435,7 @@ size_t real_partial_words(int cap) { return (size_t)((cap + 31) / 32 + 1) * kRea
 int launch_real_space(const Geom &coarse, const double L[6], int n, const double *x, const double *w, float eta,
                       float rcut, SortBuffers &sb, double4 *rec, float4 *tab, double *dx, double *partials,
                       double eta_d, double *out, cudaStream_t st) {
-  int k = launch_cell_sort(coarse, n, x, w, sb, st);
+  int k = launch_cell_sort(coarse, n, x, w, sb, st, 0);  // one bucket per coarse cell
   const int ngroups = (n + 31) / 32;
   if (n > 0) {
     int *cellc = reinterpret_cast<int *>(rec);  // rec holds n ints here

@@ -3,8 +3,9 @@
 // The reference inserts every atom into a std::multimap keyed by
 // cid = (n0*K1 + n1)*K2 + n2; equal keys keep insertion order, so the result
 // is the STABLE sort of atoms by cid.  Two sorts produce that order here:
-//   - the main path (launch_cell_sort, below) is a counting sort over the
-//     cells, which also yields the per-cell offsets the spread needs;
+//   - the main path (launch_cell_sort, below) is a counting sort over
+//     buckets of cells (runs of z cells of one cell row), which also yields
+//     the per-bucket offsets the spread and the real-space walk need;
 //   - the allocation-free entry point (end of file) is an LSD radix sort
 //     whose scratch is bounded by the atom count:
 //       1. key_hist_kernel: FP64 cell keys (rounding identical to the host,
@@ -198,29 +199,36 @@ static int key_passes(long ncell) {
 }
 
 // ---------------------------------------------------------------------------
-// Main-path cell sort: a counting sort over the cells.
+// Main-path cell sort: a counting sort over buckets of cells.
+//
+// A bucket is a run of 2^zshift consecutive z cells of one (x, y) cell row:
+// bucket = (n0 K1 + n1) nzb + (n2 >> zshift), nzb = ceil(K2 / 2^zshift), so
+// buckets are ordered like the keys they hold.  zshift = 0 gives one bucket
+// per cell (the real-space cell list needs per-cell offsets); the spread
+// takes runs of 32 cells, which keeps the count array at K0 K1 K2 / 32 words
+// (2 MB at 256^3 instead of 67 MB), resident in L2.
 //
 //   1. key_count_kernel: keys and records (as above); every atom takes an
-//      arrival slot in its cell with an integer atomic (count[key]++).
-//   2. tile_sum_kernel + cell_offsets_kernel: exclusive scan of the per-cell
-//      counts, in place, into cell_start (cell_start[ncell] = n): the sum of
-//      every tile of 2^tshift cells, then each tile scans its cells from the
-//      sum of the tiles before it (at most ~2048 tiles, so that sum is short).
-//   3. cell_scatter_kernel: every atom goes to cell_start[key] + its arrival
-//      slot.  A cell holding one atom is final; the atoms of a shared cell
-//      sit in arrival order, which is not deterministic.
-//   4. cell_fixup_kernel: the atoms of each shared cell are put in input
-//      order (rank = number of the cell's atoms with a smaller index), which
-//      is exactly the stable order of the reference's multimap.  Cells with
-//      more than kBigCell atoms are listed and merge-sorted by the last CTA
-//      to finish (no waiting on other CTAs).
+//      arrival slot in its bucket with an integer atomic (count[bucket]++).
+//   2. tile_sum_kernel + cell_offsets_kernel: exclusive scan of the
+//      per-bucket counts, in place, into cell_start (cell_start[nb] = n):
+//      the sum of every tile of 2^tshift buckets, then each tile scans its
+//      buckets from the sum of the tiles before it (at most ~2048 tiles).
+//   3. cell_scatter_kernel: every atom goes to cell_start[bucket] + its
+//      arrival slot, with its key; an atom alone in its bucket is final.
+//   4. cell_fixup_kernel: the atoms of each shared bucket are put in
+//      (key, input index) order -- rank = number of the bucket's atoms with a
+//      smaller (key, index) pair -- which is exactly the stable order of the
+//      reference's multimap.  Buckets with more than kBigCell atoms are
+//      listed and merge-sorted by the last CTA to finish (no waiting on other
+//      CTAs).
 // Only integer atomics (counts) are used; the result is the same bits on
 // every run.
 
 constexpr int kBigCell = 256;
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 16;
-constexpr int kScanChunk = kScanThreads * kScanItems;  // cells per CTA pass
+constexpr int kScanChunk = kScanThreads * kScanItems;  // buckets per CTA pass
 
 static int cell_tile_shift(long ncell) {
   int s = 13;  // log2(kScanChunk)
@@ -232,17 +240,41 @@ static long cell_tiles(long ncell) {
   return (ncell + 1 + (1L << s) - 1) >> s;
 }
 
-// Word layout of the cell-count region (the counts and the two control
+long sort_buckets(const Geom &g, int zshift) {
+  const long nzb = ((long)g.K2 + (1L << zshift) - 1) >> zshift;
+  return (long)g.K0 * g.K1 * nzb;
+}
+
+// Word layout of the bucket-count region (the counts and the two control
 // words are zeroed before every sort):
-//   [0, ncell + 1)           counts, then offsets
-//   [ncell + 1, ncell + 3)   control: large cells, finished fix-up CTAs
-//   [ncell + 3, + T)         tile sums
-size_t cell_count_words(long ncell) { return (size_t)(ncell + 3 + cell_tiles(ncell)); }
+//   [0, nb + 1)           counts, then offsets
+//   [nb + 1, nb + 3)      control: large buckets, finished fix-up CTAs
+//   [nb + 3, + T)         tile sums
+size_t cell_count_words(long nb) { return (size_t)(nb + 3 + cell_tiles(nb)); }
+
+// Bucket of a cell key (see above).
+struct BucketMap {
+  FastDiv K2d;
+  uint32_t nzb, zshift;
+  __device__ __forceinline__ uint32_t operator()(uint32_t key) const {
+    uint32_t row, n2;
+    K2d.divmod(key, row, n2);
+    return row * nzb + (n2 >> zshift);
+  }
+};
+
+static BucketMap bucket_map(const Geom &g, int zshift) {
+  BucketMap m;
+  m.K2d = FastDiv((uint32_t)g.K2);
+  m.nzb = (uint32_t)(((long)g.K2 + (1L << zshift) - 1) >> zshift);
+  m.zshift = (uint32_t)zshift;
+  return m;
+}
 
 __global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const double *__restrict__ x,
                                                         const double *__restrict__ w, uint32_t *__restrict__ keys,
                                                         uint32_t *__restrict__ slot, float4 *__restrict__ rec,
-                                                        uint32_t *__restrict__ count) {
+                                                        uint32_t *__restrict__ count, BucketMap bm) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   const CellConst cc = *g.cell;
@@ -250,7 +282,7 @@ __global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const dou
   const uint32_t key = cell_key(g, cc, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
   keys[a] = key;
   rec[a] = r;
-  slot[a] = atomicAdd(&count[key], 1u);
+  slot[a] = atomicAdd(&count[bm(key)], 1u);
 }
 
 // Block-wide sum (every thread gets the result); red: one word per warp.
@@ -283,7 +315,7 @@ __device__ __forceinline__ bool load_counts(const uint32_t *cs, long c, long nsc
   return full;
 }
 
-// tsum[t] = sum of the counts of tile t (cells [t << tshift, (t + 1) << tshift)).
+// tsum[t] = sum of the counts of tile t (buckets [t << tshift, (t + 1) << tshift)).
 __global__ void __launch_bounds__(kScanThreads) tile_sum_kernel(const uint32_t *__restrict__ cs, long nscan,
                                                                 int tshift, uint32_t *__restrict__ tsum) {
   __shared__ uint32_t red[kScanThreads / 32];
@@ -300,8 +332,8 @@ __global__ void __launch_bounds__(kScanThreads) tile_sum_kernel(const uint32_t *
   if (threadIdx.x == 0) tsum[blockIdx.x] = s;
 }
 
-// cs[0 .. nscan): per-cell counts in, exclusive prefix sums out, one CTA per
-// tile; the tile's base is the sum of the earlier tiles' sums.
+// cs[0 .. nscan): per-bucket counts in, exclusive prefix sums out, one CTA
+// per tile; the tile's base is the sum of the earlier tiles' sums.
 __global__ void __launch_bounds__(kScanThreads) cell_offsets_kernel(uint32_t *__restrict__ cs, long nscan,
                                                                     int tshift, const uint32_t *__restrict__ tsum) {
   constexpr int NW = kScanThreads / 32;
@@ -356,80 +388,94 @@ __global__ void __launch_bounds__(kScanThreads) cell_offsets_kernel(uint32_t *__
   }
 }
 
+// Atom a -> offset of its bucket + its arrival slot.  Every atom leaves its
+// key and index there in tkeys/tmp (arrival order); an atom alone in its
+// bucket is already final (skeys, perm, rec_sorted).
 __global__ void __launch_bounds__(256) cell_scatter_kernel(int n, const uint32_t *__restrict__ keys,
                                                            const uint32_t *__restrict__ slot,
                                                            const float4 *__restrict__ rec,
-                                                           const int *__restrict__ cs, uint32_t *__restrict__ skeys,
-                                                           uint32_t *__restrict__ perm, uint32_t *__restrict__ tmp,
+                                                           const int *__restrict__ cs, BucketMap bm,
+                                                           uint32_t *__restrict__ skeys, uint32_t *__restrict__ perm,
+                                                           uint32_t *__restrict__ tkeys, uint32_t *__restrict__ tmp,
                                                            float4 *__restrict__ rec_sorted) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   const uint32_t key = keys[a];
-  const int lo = cs[key], hi = cs[key + 1];
+  const uint32_t b = bm(key);
+  const int lo = cs[b], hi = cs[b + 1];
   const int pos = lo + (int)slot[a];
-  skeys[pos] = key;
+  tkeys[pos] = key;
+  tmp[pos] = (uint32_t)a;
   if (hi - lo == 1) {
+    skeys[pos] = key;
     perm[pos] = (uint32_t)a;
     rec_sorted[pos] = rec[a];
-  } else {
-    tmp[pos] = (uint32_t)a;
   }
 }
 
-// Merge sort of one large cell's atom indices (distinct values) by one CTA,
-// ping-ponging between tmp[lo..) and perm[lo..); then the records.
-__device__ void big_cell_sort(int lo, int c, uint32_t *tmp, uint32_t *perm, const float4 *__restrict__ rec,
-                              float4 *__restrict__ rec_sorted) {
-  uint32_t *src = tmp + lo, *dst = perm + lo;
+__device__ __forceinline__ bool pair_less(uint32_t ka, uint32_t ia, uint32_t kb, uint32_t ib) {
+  return ka < kb || (ka == kb && ia < ib);
+}
+
+// Merge sort of one large bucket's (key, index) pairs (distinct pairs) by
+// one CTA, ping-ponging between (tkeys, tmp)[lo..) and (skeys, perm)[lo..);
+// then the records.
+__device__ void big_cell_sort(int lo, int c, uint32_t *tkeys, uint32_t *tmp, uint32_t *skeys, uint32_t *perm,
+                              const float4 *__restrict__ rec, float4 *__restrict__ rec_sorted) {
+  uint32_t *sk = tkeys + lo, *si = tmp + lo, *dk = skeys + lo, *di = perm + lo;
   for (int wd = 1; wd < c; wd <<= 1) {
     for (int i = threadIdx.x; i < c; i += blockDim.x) {
       const int run = i / wd, rs = run * wd;
       const bool left = (run & 1) == 0;
       const int os = left ? rs + wd : rs - wd;  // partner run
       const int oe = min(os + wd, c);
-      const uint32_t v = src[i];
-      int l = os, h = (os < c) ? oe : os;  // number of partner values below v
+      const uint32_t vk = sk[i], vi = si[i];
+      int l = os, h = (os < c) ? oe : os;  // number of partner pairs below (vk, vi)
       while (l < h) {
         const int m = (l + h) >> 1;
-        if (src[m] < v) l = m + 1; else h = m;
+        if (pair_less(sk[m], si[m], vk, vi)) l = m + 1; else h = m;
       }
-      dst[(left ? rs : os) + (i - rs) + (l - os)] = v;
+      const int d = (left ? rs : os) + (i - rs) + (l - os);
+      dk[d] = vk;
+      di[d] = vi;
     }
     __syncthreads();
-    uint32_t *t = src;
-    src = dst;
-    dst = t;
+    uint32_t *t = sk; sk = dk; dk = t;
+    t = si; si = di; di = t;
   }
   for (int i = threadIdx.x; i < c; i += blockDim.x) {
-    const uint32_t a = src[i];
+    const uint32_t k = sk[i], a = si[i];
+    skeys[lo + i] = k;
     perm[lo + i] = a;
     rec_sorted[lo + i] = rec[a];
   }
   __syncthreads();
 }
 
-// ctl[0]: number of listed large cells, ctl[1]: finished CTAs (both zero on
-// entry; the last CTA resets ctl[1]).  big: listed cell keys (capacity n).
-__global__ void __launch_bounds__(256) cell_fixup_kernel(int n, const uint32_t *__restrict__ skeys,
-                                                         const int *__restrict__ cs, uint32_t *tmp, uint32_t *perm,
-                                                         const float4 *__restrict__ rec,
+// ctl[0]: number of listed large buckets, ctl[1]: finished CTAs (both zero on
+// entry; the last CTA resets ctl[1]).  big: listed bucket indices (capacity n).
+__global__ void __launch_bounds__(256) cell_fixup_kernel(int n, const int *__restrict__ cs, BucketMap bm,
+                                                         uint32_t *tkeys, uint32_t *tmp, uint32_t *skeys,
+                                                         uint32_t *perm, const float4 *__restrict__ rec,
                                                          float4 *__restrict__ rec_sorted, uint32_t *ctl,
                                                          uint32_t *big) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
-    const uint32_t key = skeys[i];
-    const int lo = cs[key], c = cs[key + 1] - lo;
+    const uint32_t key = tkeys[i];
+    const uint32_t b = bm(key);
+    const int lo = cs[b], c = cs[b + 1] - lo;
     if (c > kBigCell) {
-      if (i == lo) big[atomicAdd(&ctl[0], 1u)] = key;
+      if (i == lo) big[atomicAdd(&ctl[0], 1u)] = b;
     } else if (c > 1) {
       const uint32_t a = tmp[i];
       int r = 0;
-      for (int j = lo; j < lo + c; j++) r += (tmp[j] < a) ? 1 : 0;
+      for (int j = lo; j < lo + c; j++) r += pair_less(tkeys[j], tmp[j], key, a) ? 1 : 0;
+      skeys[lo + r] = key;
       perm[lo + r] = a;
       rec_sorted[lo + r] = rec[a];
     }
   }
-  // the last CTA to finish sorts the listed large cells
+  // the last CTA to finish sorts the listed large buckets
   __shared__ bool last;
   __threadfence();
   __syncthreads();
@@ -438,40 +484,42 @@ __global__ void __launch_bounds__(256) cell_fixup_kernel(int n, const uint32_t *
   if (!last) return;
   __threadfence();
   const uint32_t nb = *((volatile uint32_t *)&ctl[0]);
-  for (uint32_t b = 0; b < nb; b++) {
-    const uint32_t key = *((volatile uint32_t *)&big[b]);
-    const int lo = cs[key], c = cs[key + 1] - lo;
-    big_cell_sort(lo, c, tmp, perm, rec, rec_sorted);
+  for (uint32_t k = 0; k < nb; k++) {
+    const uint32_t b = *((volatile uint32_t *)&big[k]);
+    const int lo = cs[b], c = cs[b + 1] - lo;
+    big_cell_sort(lo, c, tkeys, tmp, skeys, perm, rec, rec_sorted);
   }
   if (threadIdx.x == 0) ctl[1] = 0u;
 }
 
-// Computes keys/fractions, sorts, and builds the per-cell offsets.
+// Computes keys/fractions, sorts, and builds the per-bucket offsets.
 // On return (stream order): keys[0] / vals[0] hold the stable order,
-// rec_sorted the records in that order, cell_start the cell offsets.
-int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
-                     cudaStream_t st) {
-  const long ncell = (long)g.K0 * g.K1 * g.K2;
-  const long ntiles = cell_tiles(ncell);
-  const int tshift = cell_tile_shift(ncell);
+// rec_sorted the records in that order, cell_start the bucket offsets
+// (sort_buckets(g, zshift) + 1 of them).
+int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b, cudaStream_t st,
+                     int zshift) {
+  const long nb = sort_buckets(g, zshift);
+  const long ntiles = cell_tiles(nb);
+  const int tshift = cell_tile_shift(nb);
+  const BucketMap bm = bucket_map(g, zshift);
   uint32_t *count = reinterpret_cast<uint32_t *>(b.cell_start);
-  uint32_t *ctl = count + (ncell + 1);
-  uint32_t *tsum = count + (ncell + 3);
+  uint32_t *ctl = count + (nb + 1);
+  uint32_t *tsum = count + (nb + 3);
   b.cur = 0;
-  cudaMemsetAsync(count, 0, sizeof(uint32_t) * (ncell + 3), st);
+  cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nb + 3), st);
   int launches = 0;
   if (n > 0) {
-    key_count_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[1], b.vals[1], b.rec, count);
+    key_count_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[1], b.vals[1], b.rec, count, bm);
     launches++;
   }
-  tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, ncell + 1, tshift, tsum);
-  cell_offsets_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, ncell + 1, tshift, tsum);
+  tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);
+  cell_offsets_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);
   launches += 2;
   if (n > 0) {
-    cell_scatter_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[1], b.vals[1], b.rec, b.cell_start, b.keys[0],
-                                                          b.vals[0], b.tmp, b.rec_sorted);
-    cell_fixup_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[0], b.cell_start, b.tmp, b.vals[0], b.rec,
-                                                        b.rec_sorted, ctl, b.hist);
+    cell_scatter_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[1], b.vals[1], b.rec, b.cell_start, bm,
+                                                          b.keys[0], b.vals[0], b.tkeys, b.tmp, b.rec_sorted);
+    cell_fixup_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.cell_start, bm, b.tkeys, b.tmp, b.keys[0], b.vals[0],
+                                                        b.rec, b.rec_sorted, ctl, b.hist);
     launches += 2;
   }
   return launches;

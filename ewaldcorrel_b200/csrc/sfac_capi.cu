@@ -188,6 +188,7 @@ void free_real(Handle *h) {
     dfree(r.sb.vals[i]);
   }
   dfree(r.sb.tmp);
+  dfree(r.sb.tkeys);
   dfree(r.sb.rec);
   dfree(r.sb.rec_sorted);
   dfree(r.sb.hist);
@@ -211,7 +212,8 @@ bool ensure_real(Handle *h, int n, long ncell) {
   free_real(h);
   bool ok = true;
   for (int i = 0; i < 2 && ok; i++) ok = dalloc(h, &r.sb.keys[i], cap) && dalloc(h, &r.sb.vals[i], cap);
-  ok = ok && dalloc(h, &r.sb.tmp, cap) && dalloc(h, &r.sb.rec, cap) && dalloc(h, &r.sb.rec_sorted, cap) &&
+  ok = ok && dalloc(h, &r.sb.tmp, cap) && dalloc(h, &r.sb.tkeys, cap) && dalloc(h, &r.sb.rec, cap) &&
+       dalloc(h, &r.sb.rec_sorted, cap) &&
        dalloc(h, &r.sb.hist, cap) && dalloc(h, &r.sb.cell_start, cell_count_words(ncell)) &&
        dalloc(h, &r.rec, cap) && dalloc(h, &r.x, 3 * (size_t)cap) && dalloc(h, &r.w, cap) &&
        dalloc(h, &r.dx, 3 * (size_t)cap) && dalloc(h, &r.part, real_partial_words(cap)) && dalloc(h, &r.out, 16) &&
@@ -233,6 +235,7 @@ void free_atoms(Handle *h) {
     dfree(h->sb.vals[i]);
   }
   dfree(h->sb.tmp);
+  dfree(h->sb.tkeys);
   dfree(h->sb.rec);
   dfree(h->sb.rec_sorted);
   dfree(h->sb.hist);
@@ -245,7 +248,8 @@ bool ensure_atoms(Handle *h, int n) {
   const int cap = n + n / 2 + 64;
   bool ok = dalloc(h, &h->d_x, 3 * (size_t)cap) && dalloc(h, &h->d_w, cap);
   for (int i = 0; i < 2; i++) ok = ok && dalloc(h, &h->sb.keys[i], cap) && dalloc(h, &h->sb.vals[i], cap);
-  ok = ok && dalloc(h, &h->sb.tmp, cap) && dalloc(h, &h->sb.rec, cap) && dalloc(h, &h->sb.rec_sorted, cap) &&
+  ok = ok && dalloc(h, &h->sb.tmp, cap) && dalloc(h, &h->sb.tkeys, cap) && dalloc(h, &h->sb.rec, cap) &&
+       dalloc(h, &h->sb.rec_sorted, cap) &&
        dalloc(h, &h->sb.hist, cap);
   if (!ok) {
     free_atoms(h);
@@ -372,6 +376,7 @@ void *sfac_ctor(double L[6], int K[3], int order) {
   g.order = order;
   make_spline(order, h->spline, h->nodes);
   fft_prepare_kernels();
+  spread_prepare();
   if (const char *e = getenv("SFAC_NO_GRAPH")) h->use_graph = !(e[0] && e[0] != '0');
   if (const char *e = getenv("SFAC_ZY_MODE")) {
     const int v = atoi(e);
@@ -388,7 +393,7 @@ void *sfac_ctor(double L[6], int K[3], int order) {
                   kRedWords) &&
        dalloc(h, &h->d_red, kRedWords) && dalloc(h, &h->d_ev, kRedWords) && dalloc(h, &h->d_cell, 1) &&
        dalloc(h, &h->d_ic, 1) &&
-       dalloc(h, &h->sb.cell_start, cell_count_words(ncell));
+       dalloc(h, &h->sb.cell_start, cell_count_words(sort_buckets(g, kSpreadZShift)));
   for (int d = 0; d < 3 && ok; d++) ok = dalloc(h, &h->d_iB[d], K[d]) && dalloc(h, &h->d_tw[d], K[d]);
   const size_t hf = (size_t)(2 * h->nmodes > h->nreal ? 2 * h->nmodes : h->nreal);
   ok = ok && CK(h, cudaMallocHost((void **)&h->h_S, sizeof(double) * 2 * h->nmodes)) &&
@@ -432,7 +437,7 @@ void sfac(void *p, int n, const double *w, const double *x) {
       return;
   }
   CK(h, cudaEventRecord(h->ev_in, h->stream));
-  int k = launch_cell_sort(h->geom, n, h->d_x, h->d_w, h->sb, h->stream);
+  int k = launch_cell_sort(h->geom, n, h->d_x, h->d_w, h->sb, h->stream, kSpreadZShift);
   k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real,
                      h->stream);
   DeconvArgs dc{h->d_iB[0], h->d_iB[1], h->d_iB[2], h->ldim};
@@ -954,7 +959,7 @@ static int enqueue_solve(Handle *h, int n, const double *x, const double *w, dou
   cudaStream_t st = h->stream;
   int k = 0;
   if (timed) CK(h, cudaEventRecord(h->ev_stage[0], st));
-  k += launch_cell_sort(h->geom, n, x, w, h->sb, st);
+  k += launch_cell_sort(h->geom, n, x, w, h->sb, st, kSpreadZShift);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[1], st));
   k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real, st);
   if (timed) CK(h, cudaEventRecord(h->ev_stage[2], st));
@@ -1076,10 +1081,11 @@ int sfac_set_tuning(void *p, int key, int value) {
 unsigned long sfac_footprint_bytes(const int K[3], int n) {
   const size_t K0 = K[0], K1 = K[1], K2 = K[2], ldim = K2 / 2 + 1, nn = (size_t)(n > 0 ? n : 1);
   const size_t cap = nn + nn / 2 + 64;
-  size_t b = 4 * K0 * K1 * K2 + 8 * K0 * K1 * ldim + 4 * cell_count_words((long)(K0 * K1 * K2));  // grids, cells
+  const long nzb = ((long)K2 + (1L << kSpreadZShift) - 1) >> kSpreadZShift;
+  size_t b = 4 * K0 * K1 * K2 + 8 * K0 * K1 * ldim + 4 * cell_count_words((long)(K0 * K1) * nzb);  // grids, buckets
   b += (K0 + K1 + K2) * 16 + sizeof(RowImg) * K0 * K1;                   // moduli, twiddles, rows
   b += 8 * (size_t)fft_x_blocks_max(K[1], K[2]) * kRedWords;               // partials
-  b += cap * (24 + 8 + 6 * 4 + 16 + 16);                                   // sort buffers, records
+  b += cap * (24 + 8 + 7 * 4 + 16 + 16);                                   // sort buffers, records
   b += 8 * cap * 8;                                                        // gather staging
   b += 8 * 2 * K0 * K1 * ldim + 4 * K0 * K1 * K2;                          // host mirrors (pinned)
   return b;

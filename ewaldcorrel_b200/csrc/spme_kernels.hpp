@@ -12,21 +12,28 @@ namespace spme {
 // ---- sort (k_sort.cu) ----
 struct SortBuffers {
   uint32_t *keys[2];   // [1]: cell key of every atom (input order); [0]: keys in cell order
-  uint32_t *vals[2];   // [1]: arrival slot of every atom in its cell; [0]: the stable permutation
-  uint32_t *tmp;       // cell-order slots of shared cells, in arrival order (cap)
+  uint32_t *vals[2];   // [1]: arrival slot of every atom in its bucket; [0]: the stable permutation
+  uint32_t *tkeys;     // keys in bucket-offset + arrival-slot order (cap)
+  uint32_t *tmp;       // atom indices in the same order (cap)
   float4 *rec;         // (frac0, frac1, frac2, charge) in input order (cap)
   float4 *rec_sorted;  // the same in cell order (cap)
-  uint32_t *hist;      // keys of cells too large for the in-place fix-up (cap)
-  int *cell_start;     // cell_count_words(ncell): K0*K1*K2 + 1 counts -> offsets, tile counts, control words
+  uint32_t *hist;      // buckets too large for the in-place fix-up (cap)
+  int *cell_start;     // cell_count_words(nb): nb + 1 bucket counts -> offsets, tile counts, control words
   int cur;             // which keys/vals buffer holds the sorted result (0)
 };
-size_t cell_count_words(long ncell);
-int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b,
-                      cudaStream_t st);
+// Buckets of the sort: runs of 2^zshift z cells of each (x, y) cell row.
+// The spread's bucket: 32 z cells (its bricks are 32 points deep in z).
+constexpr int kSpreadZShift = 5;
+long sort_buckets(const Geom &g, int zshift);
+size_t cell_count_words(long nbuckets);
+int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, SortBuffers &b, cudaStream_t st,
+                     int zshift);
 
 // ---- spread (k_spread.cu) ----
+// cell_start: the bucket offsets of a launch_cell_sort with kSpreadZShift.
 int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
                   const float4 *rec_sorted, float *grid, cudaStream_t st);
+void spread_prepare();  // sets the spread's shared-memory limit once (before any graph capture)
 
 struct Influence;  // defined below (influence function source)
 
