@@ -14,17 +14,16 @@
 // (x, y) cell rows, found through the bucket offsets of the cell sort (runs
 // of 32 z cells per row) and trimmed to the halo's z cells by a search on the
 // sorted keys.  They are staged 32 at a time, one per lane: the order-p
-// B-spline weights of the three fractions (the charge folded into x) are
-// written to shared memory as zero-padded rows, so that every lane reads its
-// own column's weight at a per-atom offset without a range test; the z taps
-// are stored as duplicated pairs, ready for the packed FMA.  The walk then
-// costs per atom: one broadcast load of its offsets and window case, the
-// lane's x-pair and y weights, one packed multiply, the z taps, and one
-// jump (the window's place in the brick is the same for every lane, so it
-// selects an unrolled code path, not a divergent branch) into p packed
-// FMAs.  Small grids split one brick's atoms over 2 or 4 warps (equal
-// contiguous shares, summed in warp order through shared memory: still a
-// fixed order).
+// B-spline taps of the three fractions (the charge folded into x), the z taps
+// as duplicated pairs ready for the packed FMA.  A branch-free pass then
+// forms each lane's two column weights wx * wy for every staged atom (a tap
+// index outside [0, p) weighs zero).  The walk goes window case by window
+// case -- the place of the atom's z taps in the brick, the same for every
+// lane -- in a compile-time unrolled chain: each case present in the chunk
+// takes its atoms from a warp ballot and adds them with p packed FMAs into
+// fixed registers, so there is no indirect jump and no divergent branch.
+// Small grids split one brick's atoms over 2 or 4 warps (equal contiguous
+// shares, summed in warp order through shared memory: still a fixed order).
 #include "spme_kernels.hpp"
 
 namespace spme {
@@ -61,10 +60,6 @@ struct SpCfg {
   // halo cell rows of a brick: cells [x0 - H, x0 + TX - 2 + H] (RX of them)
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
   static constexpr int NC = SP_TZ + P - 1;  // window cases: first z tap rz in [1 - P, TZ - 1]
-  // Tap rows: tap i of an atom sits at [OFF + i]; a lane reads [off + col]
-  // with off = OFF + P - 1 - (the atom's halo row), which stays in [1, P + 14].
-  static constexpr int OFF = 8;
-  static constexpr int WL = (P + 15) | 1;
   static constexpr int ZL = (P + 1) / 2 * 2;  // z pairs per atom (even: rows stay 16-byte aligned)
 };
 
@@ -74,9 +69,10 @@ template <int P>
 struct SpStage {
   using C = SpCfg<P>;
   f2r zp[32][C::ZL];   // (wz[t], wz[t]), t < P: weight of z = rz + t
-  f2r wxp[32][C::WL];  // (w[j], w[j + 1]) of the zero-padded x taps, charge included
-  f2r wyd[32][C::WL];  // (w[j], w[j]) of the zero-padded y taps
-  int4 meta[32];       // x pair offset, y offset, window case
+  f2r wxc[32][P + 1];  // (w[j - 1], w[j]), j = 0..P, of the x taps (charge included; w[-1] = w[P] = 0)
+  float wyc[32][9];    // y taps (odd row stride: conflict-free staging stores)
+  int2 off[32];        // (P - 1 - rx, P - 1 - ry): tap index of column 0 / row 0 of the brick
+  f2r wxy[32][32];     // [atom][lane]: the lane's two column weights wx * wy
 };
 template <int P>
 struct SpGroup {  // per brick: the halo rows' atom ranges of one z piece
@@ -103,30 +99,42 @@ __device__ __forceinline__ void sp_taps(f2r (&acc)[SP_TZ], f2r wxy, const f2r (&
   }
 }
 
-#define SPC(C)                                                     \
-  case C:                                                          \
-    if constexpr (C < SpCfg<P>::NC) sp_taps<P, C>(acc, wxy, zp);   \
-    break;
-
-template <int P>
-__device__ __forceinline__ void sp_dispatch(int c, f2r (&acc)[SP_TZ], f2r wxy, const f2r (&zp)[SpCfg<P>::ZL]) {
-  switch (c) {
-    SPC(0) SPC(1) SPC(2) SPC(3) SPC(4) SPC(5) SPC(6) SPC(7) SPC(8) SPC(9)
-    SPC(10) SPC(11) SPC(12) SPC(13) SPC(14) SPC(15) SPC(16) SPC(17) SPC(18) SPC(19)
-    SPC(20) SPC(21) SPC(22) SPC(23) SPC(24) SPC(25) SPC(26) SPC(27) SPC(28) SPC(29)
-    SPC(30) SPC(31) SPC(32) SPC(33) SPC(34) SPC(35) SPC(36) SPC(37) SPC(38)
-    default: break;
+// The walk over one staged chunk, window case by window case: case C (all
+// compile-time, so every accumulator index is fixed) takes the chunk's atoms
+// whose first z tap is C - (P - 1), in lane order, from a warp ballot.  No
+// indirect jump: a case absent from the chunk costs one uniform test.
+template <int P, int C>
+__device__ __forceinline__ void sp_walk(f2r (&acc)[SP_TZ], const SpStage<P> &st, int lane, int mycase,
+                                        uint32_t plo, uint32_t phi) {
+  if constexpr (C < SpCfg<P>::NC) {
+    const uint32_t bit = C < 32 ? (plo >> (C & 31)) : (phi >> (C & 31));
+    if (bit & 1u) {
+      uint32_t am = __ballot_sync(0xffffffffu, mycase == C);
+      while (am) {
+        const int a = __ffs(am) - 1;
+        am &= am - 1u;
+        const f2r wxy = st.wxy[a][lane];
+        f2r zp[SpCfg<P>::ZL];
+#pragma unroll
+        for (int v = 0; v < SpCfg<P>::ZL / 2; v++) {
+          const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zp[a][2 * v]);
+          zp[2 * v] = q.x;
+          zp[2 * v + 1] = q.y;
+        }
+        sp_taps<P, C>(acc, wxy, zp);
+      }
+    }
+    sp_walk<P, C + 1>(acc, st, lane, mycase, plo, phi);
   }
 }
-#undef SPC
-static_assert(SP_MAXC <= 39, "window cases");
 
-// Barrier of the nsplit warps that share one brick (named barrier 1 + group).
-__device__ __forceinline__ void group_sync(int group, int nsplit) {
-  if (nsplit == 1) {
+// Barrier of the NS warps that share one brick (named barrier 1 + group).
+template <int NS>
+__device__ __forceinline__ void group_sync(int group) {
+  if constexpr (NS == 1) {
     __syncwarp();
   } else {
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(32 * nsplit) : "memory");
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "n"(32 * NS) : "memory");
   }
 }
 
@@ -145,18 +153,18 @@ struct SpArgs {
   const uint32_t *keys;   // sorted cell keys
   const float4 *rec;      // sorted (fx, fy, fz, q)
   float *grid;
-  int ntx, nty, ntz, nbricks, nsplit;
+  int ntx, nty, ntz, nbricks;
   int nzb, zshift;
   FastDiv K2d;
 };
 
-template <int P>
+template <int P, int NS>
 __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spline S) {
   using C = SpCfg<P>;
-  constexpr int H = C::H, RY = C::RY, NR = C::NR, WL = C::WL, OFF = C::OFF;
+  constexpr int H = C::H, RY = C::RY, NR = C::NR;
   extern __shared__ __align__(16) unsigned char sp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nsplit = A.nsplit;
+  constexpr int nsplit = NS;
   const int group = warp / nsplit, member = warp % nsplit;
   SpStage<P> &st = *reinterpret_cast<SpStage<P> *>(sp_smem + warp * sp_stage_bytes<P>());
   SpGroup<P> &gr = *reinterpret_cast<SpGroup<P> *>(sp_smem + SP_WARPS * sp_stage_bytes<P>() +
@@ -170,14 +178,6 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
   const int lx = lane & 3, ly = lane >> 2;
   const int gt = member * 32 + lane, gn = 32 * nsplit;  // thread index and size of the group
 
-  // zero the padded tap rows once (staging overwrites only the tap positions;
-  // wxp and wyd are adjacent)
-  {
-    f2r *p = &st.wxp[0][0];
-    for (int i = lane; i < 2 * 32 * WL; i += 32) p[i] = 0ull;
-  }
-  __syncwarp();
-
   f2r acc[SP_TZ];
 #pragma unroll
   for (int z = 0; z < SP_TZ; z++) acc[z] = 0ull;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
   for (int ezs = ez_lo; ezs <= ez_hi;) {
     const int n2a = imod(ezs, K2);
     const int len = min(ez_hi - ezs + 1, K2 - n2a);
-    group_sync(group, nsplit);  // the previous piece's ranges are no longer read
+    group_sync<NS>(group);  // the previous piece's ranges are no longer read
     for (int r = gt; r < NR; r += gn) {
       const int ex = x0 - H + r / RY, ey = y0 - H + r % RY;
       const int row = imod(ex, K0) * K1 + imod(ey, K1);
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
       gr.start[r] = lo;
       gr.pref[r + 1] = hi - lo;
     }
-    group_sync(group, nsplit);
+    group_sync<NS>(group);
     if (member == 0) {
       int running = 0;
       for (int c = 0; c < NR; c += 32) {
@@ -219,12 +219,13 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
       }
       if (lane == 0) gr.pref[0] = 0;
     }
-    group_sync(group, nsplit);
+    group_sync<NS>(group);
     const int total = gr.pref[NR];
     const int zoff = ezs - n2a + 1 - H - z0;  // first z tap of an atom in stored cell n2: n2 + zoff
     const int w_lo = (int)((long)total * member / nsplit), w_hi = (int)((long)total * (member + 1) / nsplit);
     for (int chunk = w_lo; chunk < w_hi; chunk += 32) {
       const int t = chunk + lane;
+      int mycase = -1;  // window case of this lane's staged atom (-1: none)
       if (t < w_hi) {
         int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
         while (lo < hi) {
@@ -242,33 +243,32 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
 #pragma unroll
         for (int i = 0; i < P; i++) {
           const float wx = u.w * bspl_eval(S, P, u.x, P - 1 - i);
-          st.wxp[lane][OFF - 1 + i] = pack2(prev, wx);
+          st.wxc[lane][i] = pack2(prev, wx);
           prev = wx;
-          const float wy = bspl_eval(S, P, u.y, P - 1 - i);
-          st.wyd[lane][OFF + i] = pack2(wy, wy);
+          st.wyc[lane][i] = bspl_eval(S, P, u.y, P - 1 - i);
           const float wz = bspl_eval(S, P, u.z, P - 1 - i);
           st.zp[lane][i] = pack2(wz, wz);
         }
-        st.wxp[lane][OFF + P - 1] = pack2(prev, 0.f);
-        st.meta[lane] = make_int4(lane * WL + OFF + P - 1 - rx, lane * WL + OFF + P - 1 - ry,
-                                  (int)n2 + zoff + P - 1, 0);
+        st.wxc[lane][P] = pack2(prev, 0.f);
+        st.off[lane] = make_int2(P - 1 - rx, P - 1 - ry);
+        mycase = (int)n2 + zoff + P - 1;  // in [0, NC): first z tap rz = mycase - (P - 1)
       }
       __syncwarp();
       const int na = min(32, w_hi - chunk);
-      const f2r *wxl = &st.wxp[0][0] + 2 * lx;
-      const f2r *wyl = &st.wyd[0][0] + ly;
+      // this lane's column weights for every staged atom (branch-free pass):
+      // columns 2 lx, 2 lx + 1 take x taps ix, ix + 1 = pair ix + 1 of wxc,
+      // row ly takes y tap iy; taps outside [0, P) weigh zero
       for (int a = 0; a < na; a++) {
-        const int4 m = st.meta[a];
-        const f2r wxy = fmul2(wxl[m.x], wyl[m.y]);
-        f2r zp[C::ZL];
-#pragma unroll
-        for (int v = 0; v < C::ZL / 2; v++) {
-          const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zp[a][2 * v]);
-          zp[2 * v] = q.x;
-          zp[2 * v + 1] = q.y;
-        }
-        sp_dispatch<P>(m.z, acc, wxy, zp);
+        const int2 o = st.off[a];
+        const int jx = o.x + 2 * lx + 1, iy = o.y + ly;
+        const f2r xp = ((unsigned)jx <= (unsigned)P) ? st.wxc[a][jx] : 0ull;
+        const float wy = ((unsigned)iy < (unsigned)P) ? st.wyc[a][iy] : 0.f;
+        st.wxy[a][lane] = fmul2(xp, pack2(wy, wy));
       }
+      const uint32_t plo = __reduce_or_sync(0xffffffffu, (mycase >= 0 && mycase < 32) ? 1u << mycase : 0u);
+      const uint32_t phi = __reduce_or_sync(0xffffffffu, mycase >= 32 ? 1u << (mycase - 32) : 0u);
+      __syncwarp();
+      sp_walk<P, 0>(acc, st, lane, mycase, plo, phi);
       __syncwarp();  // the next chunk's staging overwrites these atoms
     }
     ezs += len;
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
   // partial bricks to shared memory (over the staging rows), summed over the
   // group's warps in warp order, stored with consecutive threads on
   // consecutive z (coalesced)
-  group_sync(group, nsplit);
+  group_sync<NS>(group);
   float *part = reinterpret_cast<float *>(&st);  // [k * 32 + z][33]: column 2 lx + k of lane
 #pragma unroll
   for (int z = 0; z < SP_TZ; z++) {
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
     part[z * 33 + lane] = v0;
     part[(32 + z) * 33 + lane] = v1;
   }
-  group_sync(group, nsplit);
+  group_sync<NS>(group);
   const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * nsplit * sp_stage_bytes<P>());
   const size_t mstride = sp_stage_bytes<P>() / sizeof(float);
   for (int p = gt; p < SP_TX * SP_TY * SP_TZ; p += gn) {
@@ -300,18 +300,32 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
   }
 }
 
-template <int P>
-static void spread_p(const SpArgs &A, const Spline &S, cudaStream_t st) {
-  const int per_cta = SP_WARPS / A.nsplit;
+template <int P, int NS>
+static void spread_ps(const SpArgs &A, const Spline &S, cudaStream_t st) {
+  constexpr int per_cta = SP_WARPS / NS;
   const long ctas = (A.nbricks + per_cta - 1) / per_cta;
-  spread_kernel<P><<<(unsigned)ctas, SP_WARPS * 32, sp_smem_bytes<P>(), st>>>(A, S);
+  spread_kernel<P, NS><<<(unsigned)ctas, SP_WARPS * 32, sp_smem_bytes<P>(), st>>>(A, S);
+}
+
+template <int P>
+static void spread_p(const SpArgs &A, int nsplit, const Spline &S, cudaStream_t st) {
+  if (nsplit == 1) spread_ps<P, 1>(A, S, st);
+  else if (nsplit == 2) spread_ps<P, 2>(A, S, st);
+  else spread_ps<P, 4>(A, S, st);
+}
+
+template <int P>
+static void spread_attr() {
+  cudaFuncSetAttribute(spread_kernel<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
+  cudaFuncSetAttribute(spread_kernel<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
+  cudaFuncSetAttribute(spread_kernel<P, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
 }
 
 void spread_prepare() {
-  cudaFuncSetAttribute(spread_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<2>());
-  cudaFuncSetAttribute(spread_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<4>());
-  cudaFuncSetAttribute(spread_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<6>());
-  cudaFuncSetAttribute(spread_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<8>());
+  spread_attr<2>();
+  spread_attr<4>();
+  spread_attr<6>();
+  spread_attr<8>();
 }
 
 static int sm_count() {
@@ -345,13 +359,13 @@ int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const u
   // Split a brick's atoms over more warps while the bricks alone would not
   // fill the SMs (4 CTAs of 4 warps resident per SM).
   const long want = (long)sm_count() * 16;
-  A.nsplit = 1;
-  while (A.nsplit < SP_WARPS && (long)A.nbricks * A.nsplit < want) A.nsplit *= 2;
+  int nsplit = 1;
+  while (nsplit < SP_WARPS && (long)A.nbricks * nsplit < want) nsplit *= 2;
   switch (g.order) {
-    case 2: spread_p<2>(A, S, st); break;
-    case 4: spread_p<4>(A, S, st); break;
-    case 6: spread_p<6>(A, S, st); break;
-    case 8: spread_p<8>(A, S, st); break;
+    case 2: spread_p<2>(A, nsplit, S, st); break;
+    case 4: spread_p<4>(A, nsplit, S, st); break;
+    case 6: spread_p<6>(A, nsplit, S, st); break;
+    case 8: spread_p<8>(A, nsplit, S, st); break;
     default: return 0;
   }
   return 1;
