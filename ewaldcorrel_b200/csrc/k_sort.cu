@@ -245,12 +245,16 @@ long sort_buckets(const Geom &g, int zshift) {
   return (long)g.K0 * g.K1 * nzb;
 }
 
-// Word layout of the bucket-count region (the counts and the two control
-// words are zeroed before every sort):
-//   [0, nb + 1)           counts, then offsets
-//   [nb + 1, nb + 3)      control: large buckets, finished fix-up CTAs
-//   [nb + 3, + T)         tile sums
-size_t cell_count_words(long nb) { return (size_t)(nb + 3 + cell_tiles(nb)); }
+// Word layout of the bucket-count region (everything before the tile sums is
+// zeroed before every sort):
+//   [0, nb + 1)            counts, then offsets
+//   [nb + 1, nb + 3)       control: large buckets, finished fix-up CTAs
+//   [nb + 3, 2 nb + 3)     head: atoms of each bucket in its first H - 1 cells
+//   [2 nb + 3, 3 nb + 3)   tail: atoms of each bucket in its last H cells
+//   [3 nb + 3, + T)        tile sums
+// (head and tail: the spread's halo of an interior brick starts H cells
+// before a bucket boundary and ends H - 1 cells after one, H = order / 2.)
+size_t cell_count_words(long nb) { return (size_t)(3 * nb + 3 + cell_tiles(nb)); }
 
 // Bucket of a cell key (see above).
 struct BucketMap {
@@ -271,10 +275,13 @@ static BucketMap bucket_map(const Geom &g, int zshift) {
   return m;
 }
 
+// head/tail (may be null): see the word layout above; ht_h = H.
 __global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const double *__restrict__ x,
                                                         const double *__restrict__ w, uint32_t *__restrict__ keys,
                                                         uint32_t *__restrict__ slot, float4 *__restrict__ rec,
-                                                        uint32_t *__restrict__ count, BucketMap bm) {
+                                                        uint32_t *__restrict__ count, BucketMap bm,
+                                                        uint32_t *__restrict__ head, uint32_t *__restrict__ tail,
+                                                        int ht_h) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   const CellConst cc = *g.cell;
@@ -282,7 +289,15 @@ __global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const dou
   const uint32_t key = cell_key(g, cc, x[3 * a], x[3 * a + 1], x[3 * a + 2], r, (float)w[a]);
   keys[a] = key;
   rec[a] = r;
-  slot[a] = atomicAdd(&count[bm(key)], 1u);
+  uint32_t row, n2;
+  bm.K2d.divmod(key, row, n2);
+  const uint32_t b = row * bm.nzb + (n2 >> bm.zshift);
+  slot[a] = atomicAdd(&count[b], 1u);
+  if (head) {
+    const int off = (int)(n2 & ((1u << bm.zshift) - 1u));
+    if (off < ht_h - 1) atomicAdd(&head[b], 1u);
+    if (off >= (1 << bm.zshift) - ht_h) atomicAdd(&tail[b], 1u);
+  }
 }
 
 // Block-wide sum (every thread gets the result); red: one word per warp.
@@ -504,12 +519,15 @@ int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, Sor
   const BucketMap bm = bucket_map(g, zshift);
   uint32_t *count = reinterpret_cast<uint32_t *>(b.cell_start);
   uint32_t *ctl = count + (nb + 1);
-  uint32_t *tsum = count + (nb + 3);
+  uint32_t *head = count + (nb + 3), *tail = count + (2 * nb + 3);
+  uint32_t *tsum = count + (3 * nb + 3);
+  const int ht_h = zshift > 0 ? g.order / 2 : 0;  // head/tail counts for the spread's buckets only
   b.cur = 0;
-  cudaMemsetAsync(count, 0, sizeof(uint32_t) * (nb + 3), st);
+  cudaMemsetAsync(count, 0, sizeof(uint32_t) * ((ht_h ? 3 * nb : nb) + 3), st);
   int launches = 0;
   if (n > 0) {
-    key_count_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[1], b.vals[1], b.rec, count, bm);
+    key_count_kernel<<<ceil_div(n, 256), 256, 0, st>>>(g, n, x, w, b.keys[1], b.vals[1], b.rec, count, bm,
+                                                       ht_h ? head : nullptr, tail, ht_h);
     launches++;
   }
   tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);

@@ -12,25 +12,30 @@
 // (fma.rn.f32x2) adds an atom's z tap to both columns.  The atoms of the
 // brick's halo (the cells whose stencils reach it) are the sorted atoms of
 // (x, y) cell rows, found through the bucket offsets of the cell sort (runs
-// of 32 z cells per row) and trimmed to the halo's z cells by a search on the
-// sorted keys.  They are staged 32 at a time, one per lane: the order-p
-// B-spline taps of the three fractions (the charge folded into x), the z taps
-// as duplicated pairs ready for the packed FMA.  A branch-free pass then
-// forms each lane's two column weights wx * wy for every staged atom (a tap
-// index outside [0, p) weighs zero).  The walk goes window case by window
-// case -- the place of the atom's z taps in the brick, the same for every
-// lane -- in a compile-time unrolled chain: each case present in the chunk
-// takes its atoms from a warp ballot and adds them with p packed FMAs into
-// fixed registers, so there is no indirect jump and no divergent branch.
-// Small grids split one brick's atoms over 2 or 4 warps (equal contiguous
-// shares, summed in warp order through shared memory: still a fixed order).
+// of 32 z cells per row); an interior brick's halo starts H = p/2 cells
+// before a bucket boundary and ends H - 1 cells after one, and the sort's
+// per-bucket head/tail counts give those cuts without a search.
+//
+// The atoms are staged 32 at a time, one per lane, at the row given by a
+// counting sort of the chunk on its window case (the place of the atom's z
+// taps in the brick, the same for every lane; ties in lane order).  Staging
+// evaluates the order-p B-spline taps of the three fractions (the charge
+// folded into x) once and stores what the lanes will read: the weight of
+// each of the brick's 8 x columns (as the 4 pairs the lanes hold) and 8 y
+// rows -- zero where the atom's stencil misses -- and the z taps as
+// duplicated pairs ready for the packed FMA.  The walk goes window case by
+// window case in a compile-time unrolled chain, each case a plain loop over
+// its contiguous rows: per atom, the lane's x pair and y weight, two
+// multiplies, the z taps and p packed FMAs into fixed registers -- no
+// indirect jump, no divergent branch.  Small grids split one brick's atoms
+// over 2 or 4 warps (equal contiguous shares, summed in warp order through
+// shared memory: still a fixed order).
 #include "spme_kernels.hpp"
 
 namespace spme {
 
 constexpr int SP_TX = 8, SP_TY = 8, SP_TZ = 32;  // brick of one warp
 constexpr int SP_WARPS = 4;                     // warps per CTA
-constexpr int SP_MAXC = SP_TZ + kMaxOrder - 1;  // window cases of the largest order
 
 typedef unsigned long long f2r;  // two FP32 values in one 64-bit register (low word first)
 
@@ -48,11 +53,6 @@ __device__ __forceinline__ f2r ffma2(f2r a, f2r b, f2r c) {
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
   return d;
 }
-__device__ __forceinline__ f2r fmul2(f2r a, f2r b) {
-  f2r d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 
 template <int P>
 struct SpCfg {
@@ -60,19 +60,23 @@ struct SpCfg {
   // halo cell rows of a brick: cells [x0 - H, x0 + TX - 2 + H] (RX of them)
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
   static constexpr int NC = SP_TZ + P - 1;  // window cases: first z tap rz in [1 - P, TZ - 1]
+  // Scratch tap rows: tap i at [OFF + i], zero elsewhere; column c of the
+  // brick (0..7) reads [OFF + P - 1 - r + c] for the atom's halo row r.
+  static constexpr int OFF = 7;
+  static constexpr int SL = (P + 14) | 1;
   static constexpr int ZL = (P + 1) / 2 * 2;  // z pairs per atom (even: rows stay 16-byte aligned)
 };
 
-// Shared memory of one warp: the staged atoms during the walk, its partial
-// brick (64 x 33 floats) for the final sum.
+// Shared memory of one warp.
 template <int P>
 struct SpStage {
   using C = SpCfg<P>;
   f2r zp[32][C::ZL];   // (wz[t], wz[t]), t < P: weight of z = rz + t
-  f2r wxc[32][P + 1];  // (w[j - 1], w[j]), j = 0..P, of the x taps (charge included; w[-1] = w[P] = 0)
-  float wyc[32][9];    // y taps (odd row stride: conflict-free staging stores)
-  int2 off[32];        // (P - 1 - rx, P - 1 - ry): tap index of column 0 / row 0 of the brick
-  f2r wxy[32][32];     // [atom][lane]: the lane's two column weights wx * wy
+  f2r wxl[32][5];      // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 5 pairs)
+  float wyl[32][9];    // y weights of rows 0..7 (padded to 9)
+  int cnt[64];         // atoms per window case in the chunk, then the case starts
+  float sx[32][C::SL]; // per-lane scratch: zero-padded x taps (charge included)
+  float sy[32][C::SL]; // per-lane scratch: zero-padded y taps
 };
 template <int P>
 struct SpGroup {  // per brick: the halo rows' atom ranges of one z piece
@@ -100,31 +104,27 @@ __device__ __forceinline__ void sp_taps(f2r (&acc)[SP_TZ], f2r wxy, const f2r (&
 }
 
 // The walk over one staged chunk, window case by window case: case C (all
-// compile-time, so every accumulator index is fixed) takes the chunk's atoms
-// whose first z tap is C - (P - 1), in lane order, from a warp ballot.  No
-// indirect jump: a case absent from the chunk costs one uniform test.
+// compile-time, so every accumulator index is fixed) adds the staged rows
+// [start[C], start[C + 1]); a case absent from the chunk costs one test.
 template <int P, int C>
-__device__ __forceinline__ void sp_walk(f2r (&acc)[SP_TZ], const SpStage<P> &st, int lane, int mycase,
-                                        uint32_t plo, uint32_t phi) {
+__device__ __forceinline__ void sp_walk(f2r (&acc)[SP_TZ], const SpStage<P> &st, int lx, int ly, int k) {
   if constexpr (C < SpCfg<P>::NC) {
-    const uint32_t bit = C < 32 ? (plo >> (C & 31)) : (phi >> (C & 31));
-    if (bit & 1u) {
-      uint32_t am = __ballot_sync(0xffffffffu, mycase == C);
-      while (am) {
-        const int a = __ffs(am) - 1;
-        am &= am - 1u;
-        const f2r wxy = st.wxy[a][lane];
-        f2r zp[SpCfg<P>::ZL];
+    const int e = st.cnt[C + 1];
+#pragma unroll 1
+    for (; k < e; k++) {
+      const float2 xp = *reinterpret_cast<const float2 *>(&st.wxl[k][lx]);
+      const float wy = st.wyl[k][ly];
+      const f2r wxy = pack2(xp.x * wy, xp.y * wy);
+      f2r zp[SpCfg<P>::ZL];
 #pragma unroll
-        for (int v = 0; v < SpCfg<P>::ZL / 2; v++) {
-          const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zp[a][2 * v]);
-          zp[2 * v] = q.x;
-          zp[2 * v + 1] = q.y;
-        }
-        sp_taps<P, C>(acc, wxy, zp);
+      for (int v = 0; v < SpCfg<P>::ZL / 2; v++) {
+        const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zp[k][2 * v]);
+        zp[2 * v] = q.x;
+        zp[2 * v + 1] = q.y;
       }
+      sp_taps<P, C>(acc, wxy, zp);
     }
-    sp_walk<P, C + 1>(acc, st, lane, mycase, plo, phi);
+    sp_walk<P, C + 1>(acc, st, lx, ly, k);
   }
 }
 
@@ -147,59 +147,77 @@ __device__ __forceinline__ int keys_lower_bound(const uint32_t *__restrict__ key
   return lo;
 }
 
+// v mod K: one test each way for v in [-K, 2K) (near), the full modulus otherwise.
+__device__ __forceinline__ int wrap_near(int v, int K, bool near) {
+  if (near) return v < 0 ? v + K : (v >= K ? v - K : v);
+  return imod(v, K);
+}
+
 struct SpArgs {
   Geom g;
-  const int *cs;          // bucket offsets (runs of 2^zshift z cells per row)
+  const int *cs;          // bucket offsets (runs of 32 z cells per row)
+  const uint32_t *head;   // per bucket: atoms in its first H - 1 cells
+  const uint32_t *tail;   // per bucket: atoms in its last H cells
   const uint32_t *keys;   // sorted cell keys
   const float4 *rec;      // sorted (fx, fy, fz, q)
   float *grid;
   int ntx, nty, ntz, nbricks;
-  int nzb, zshift;
+  int nzb;
   FastDiv K2d;
 };
 
 template <int P, int NS>
-__global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spline S) {
+__global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spline S) {
   using C = SpCfg<P>;
-  constexpr int H = C::H, RY = C::RY, NR = C::NR;
+  constexpr int H = C::H, RX = C::RX, RY = C::RY, NR = C::NR, OFF = C::OFF, NC = C::NC;
+  constexpr int ZB = 5, ZW = 1 << ZB;  // bucket: 32 z cells
   extern __shared__ __align__(16) unsigned char sp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int nsplit = NS;
-  const int group = warp / nsplit, member = warp % nsplit;
+  const int group = warp / NS, member = warp % NS;
   SpStage<P> &st = *reinterpret_cast<SpStage<P> *>(sp_smem + warp * sp_stage_bytes<P>());
   SpGroup<P> &gr = *reinterpret_cast<SpGroup<P> *>(sp_smem + SP_WARPS * sp_stage_bytes<P>() +
                                                    group * sizeof(SpGroup<P>));
-  const long brick = (long)blockIdx.x * (SP_WARPS / nsplit) + group;
+  const long brick = (long)blockIdx.x * (SP_WARPS / NS) + group;
   if (brick >= A.nbricks) return;  // the whole group leaves together
   const Geom &g = A.g;
   const int K0 = g.K0, K1 = g.K1, K2 = g.K2;
   const int tz = (int)(brick % A.ntz), ty = (int)((brick / A.ntz) % A.nty), tx = (int)(brick / ((long)A.ntz * A.nty));
   const int x0 = tx * SP_TX, y0 = ty * SP_TY, z0 = tz * SP_TZ;
   const int lx = lane & 3, ly = lane >> 2;
-  const int gt = member * 32 + lane, gn = 32 * nsplit;  // thread index and size of the group
+  const int gt = member * 32 + lane, gn = 32 * NS;  // thread index and size of the group
+  const bool nearx = K0 >= RX, neary = K1 >= RY;
+
+  // zero this lane's scratch rows once (staging writes only the tap positions)
+  for (int i = 0; i < C::SL; i++) {
+    st.sx[lane][i] = 0.f;
+    st.sy[lane][i] = 0.f;
+  }
 
   f2r acc[SP_TZ];
 #pragma unroll
   for (int z = 0; z < SP_TZ; z++) acc[z] = 0ull;
 
-  const uint32_t zmask = (1u << A.zshift) - 1u;
   // extended z cells whose stencils reach [z0, z0 + TZ): [z0 - H, z0 + TZ + H - 2],
   // walked in pieces that do not cross the periodic boundary
   const int ez_lo = z0 - H, ez_hi = z0 + SP_TZ + H - 2;
   for (int ezs = ez_lo; ezs <= ez_hi;) {
     const int n2a = imod(ezs, K2);
     const int len = min(ez_hi - ezs + 1, K2 - n2a);
+    const int n2e = n2a + len;  // one past the piece's last cell
     group_sync<NS>(group);  // the previous piece's ranges are no longer read
     for (int r = gt; r < NR; r += gn) {
       const int ex = x0 - H + r / RY, ey = y0 - H + r % RY;
-      const int row = imod(ex, K0) * K1 + imod(ey, K1);
-      const int b0 = row * A.nzb + (n2a >> A.zshift), b1 = row * A.nzb + ((n2a + len - 1) >> A.zshift);
-      int lo = __ldg(A.cs + b0), hi = __ldg(A.cs + b1 + 1);
+      const int row = wrap_near(ex, K0, nearx) * K1 + wrap_near(ey, K1, neary);
+      const int b0 = row * A.nzb + (n2a >> ZB), b1 = row * A.nzb + ((n2e - 1) >> ZB);
       const uint32_t kbase = (uint32_t)row * (uint32_t)K2;
-      // trim the partial first and last buckets to cells [n2a, n2a + len)
-      if (n2a & zmask) lo = keys_lower_bound(A.keys, lo, __ldg(A.cs + b0 + 1), kbase + n2a);
-      if (((n2a + len) & zmask) && n2a + len < K2)
-        hi = keys_lower_bound(A.keys, __ldg(A.cs + b1), hi, kbase + n2a + len);
+      int lo, hi;
+      const int lo_off = n2a & (ZW - 1), hi_off = n2e & (ZW - 1);
+      if (lo_off == 0) lo = __ldg(A.cs + b0);
+      else if (lo_off == ZW - H) lo = __ldg(A.cs + b0 + 1) - (int)__ldg(A.tail + b0);
+      else lo = keys_lower_bound(A.keys, __ldg(A.cs + b0), __ldg(A.cs + b0 + 1), kbase + n2a);
+      if (hi_off == 0 || n2e == K2) hi = __ldg(A.cs + b1 + 1);
+      else if (hi_off == H - 1) hi = __ldg(A.cs + b1) + (int)__ldg(A.head + b1);
+      else hi = keys_lower_bound(A.keys, __ldg(A.cs + b1), __ldg(A.cs + b1 + 1), kbase + n2e);
       gr.start[r] = lo;
       gr.pref[r + 1] = hi - lo;
     }
@@ -222,81 +240,123 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 4) spread_kernel(SpArgs A, Spli
     group_sync<NS>(group);
     const int total = gr.pref[NR];
     const int zoff = ezs - n2a + 1 - H - z0;  // first z tap of an atom in stored cell n2: n2 + zoff
-    const int w_lo = (int)((long)total * member / nsplit), w_hi = (int)((long)total * (member + 1) / nsplit);
+    const int w_lo = (int)((long)total * member / NS), w_hi = (int)((long)total * (member + 1) / NS);
     for (int chunk = w_lo; chunk < w_hi; chunk += 32) {
       const int t = chunk + lane;
-      int mycase = -1;  // window case of this lane's staged atom (-1: none)
-      if (t < w_hi) {
+      const bool valid = t < w_hi;
+      int a = 0, hr = 0, mycase = NC;  // NC: no atom (sorts last, never walked)
+      if (valid) {
         int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
           if (gr.pref[mid] <= t) lo = mid; else hi = mid - 1;
         }
-        const int a = gr.start[lo] + (t - gr.pref[lo]);
-        const float4 u = __ldg(A.rec + a);
+        a = gr.start[lo] + (t - gr.pref[lo]);
+        hr = lo;
         uint32_t qk, n2;
         A.K2d.divmod(__ldg(A.keys + a), qk, n2);
-        const int rx = lo / RY, ry = lo % RY;
-        // tap i of each axis: the weight of point first + i, M(f + P - 1 - i);
-        // stored as soon as it is formed (the 64 accumulator registers stay live)
-        float prev = 0.f;
-#pragma unroll
-        for (int i = 0; i < P; i++) {
-          const float wx = u.w * bspl_eval(S, P, u.x, P - 1 - i);
-          st.wxc[lane][i] = pack2(prev, wx);
-          prev = wx;
-          st.wyc[lane][i] = bspl_eval(S, P, u.y, P - 1 - i);
-          const float wz = bspl_eval(S, P, u.z, P - 1 - i);
-          st.zp[lane][i] = pack2(wz, wz);
-        }
-        st.wxc[lane][P] = pack2(prev, 0.f);
-        st.off[lane] = make_int2(P - 1 - rx, P - 1 - ry);
         mycase = (int)n2 + zoff + P - 1;  // in [0, NC): first z tap rz = mycase - (P - 1)
       }
+      // counting sort of the chunk on the window case, ties in lane order:
+      // cnt[c] = atoms of case c, then (exclusive scan) the first row of case c
+      st.cnt[lane] = 0;
+      st.cnt[lane + 32] = 0;
       __syncwarp();
-      const int na = min(32, w_hi - chunk);
-      // this lane's column weights for every staged atom (branch-free pass):
-      // columns 2 lx, 2 lx + 1 take x taps ix, ix + 1 = pair ix + 1 of wxc,
-      // row ly takes y tap iy; taps outside [0, P) weigh zero
-      for (int a = 0; a < na; a++) {
-        const int2 o = st.off[a];
-        const int jx = o.x + 2 * lx + 1, iy = o.y + ly;
-        const f2r xp = ((unsigned)jx <= (unsigned)P) ? st.wxc[a][jx] : 0ull;
-        const float wy = ((unsigned)iy < (unsigned)P) ? st.wyc[a][iy] : 0.f;
-        st.wxy[a][lane] = fmul2(xp, pack2(wy, wy));
+      const uint32_t peers = __match_any_sync(0xffffffffu, mycase);
+      if (lane == __ffs(peers) - 1) st.cnt[mycase] = __popc(peers);
+      __syncwarp();
+      {
+        const int e0 = st.cnt[2 * lane], e1 = st.cnt[2 * lane + 1];
+        int incl = e0 + e1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int u = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += u;
+        }
+        __syncwarp();
+        st.cnt[2 * lane] = incl - e0 - e1;
+        st.cnt[2 * lane + 1] = incl - e1;
       }
-      const uint32_t plo = __reduce_or_sync(0xffffffffu, (mycase >= 0 && mycase < 32) ? 1u << mycase : 0u);
-      const uint32_t phi = __reduce_or_sync(0xffffffffu, mycase >= 32 ? 1u << (mycase - 32) : 0u);
       __syncwarp();
-      sp_walk<P, 0>(acc, st, lane, mycase, plo, phi);
+      if (valid) {
+        const int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
+        const float4 u = __ldg(A.rec + a);
+        // tap i of each axis: the weight of point first + i, M(f + P - 1 - i)
+#pragma unroll
+        for (int i = 0; i < P; i++) {
+          st.sx[lane][OFF + i] = u.w * bspl_eval(S, P, u.x, P - 1 - i);
+          st.sy[lane][OFF + i] = bspl_eval(S, P, u.y, P - 1 - i);
+          const float wz = bspl_eval(S, P, u.z, P - 1 - i);
+          st.zp[row][i] = pack2(wz, wz);
+        }
+        // the brick's column c takes tap c - (rx - P + 1): scratch [OFF + P - 1 - rx + c]
+        const int bx = OFF + P - 1 - hr / RY, by = OFF + P - 1 - hr % RY;
+#pragma unroll
+        for (int c = 0; c < 4; c++) st.wxl[row][c] = pack2(st.sx[lane][bx + 2 * c], st.sx[lane][bx + 2 * c + 1]);
+#pragma unroll
+        for (int c = 0; c < 8; c++) st.wyl[row][c] = st.sy[lane][by + c];
+      }
+      __syncwarp();
+      sp_walk<P, 0>(acc, st, lx, ly, 0);
       __syncwarp();  // the next chunk's staging overwrites these atoms
     }
     ezs += len;
   }
 
-  // partial bricks to shared memory (over the staging rows), summed over the
-  // group's warps in warp order, stored with consecutive threads on
-  // consecutive z (coalesced)
-  group_sync<NS>(group);
-  float *part = reinterpret_cast<float *>(&st);  // [k * 32 + z][33]: column 2 lx + k of lane
+  if constexpr (NS == 1) {
+    // one writer per brick: each lane stores its two columns from registers
 #pragma unroll
-  for (int z = 0; z < SP_TZ; z++) {
-    float v0, v1;
-    unpack2(acc[z], v0, v1);
-    part[z * 33 + lane] = v0;
-    part[(32 + z) * 33 + lane] = v1;
-  }
-  group_sync<NS>(group);
-  const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * nsplit * sp_stage_bytes<P>());
-  const size_t mstride = sp_stage_bytes<P>() / sizeof(float);
-  for (int p = gt; p < SP_TX * SP_TY * SP_TZ; p += gn) {
-    const int z = p & 31, col = p >> 5;
-    const int xr = col >> 3, yr = col & 7;
-    const int src = ((xr & 1) * 32 + z) * 33 + (xr >> 1) + 4 * yr;
-    float v = gpart[src];
-    for (int m = 1; m < nsplit; m++) v += gpart[m * mstride + src];
-    const int gx = x0 + xr, gy = y0 + yr, gz = z0 + z;
-    if (gx < K0 && gy < K1 && gz < K2) A.grid[((long)gx * K1 + gy) * K2 + gz] = v;
+    for (int c = 0; c < 2; c++) {
+      const int gx = x0 + 2 * lx + c, gy = y0 + ly;
+      if (gx >= K0 || gy >= K1) continue;
+      float *col = A.grid + ((long)gx * K1 + gy) * K2 + z0;
+      if ((K2 & 3) == 0 && z0 + SP_TZ <= K2) {
+#pragma unroll
+        for (int z = 0; z < SP_TZ; z += 4) {
+          float v[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            float lo, hi;
+            unpack2(acc[z + q], lo, hi);
+            v[q] = c ? hi : lo;
+          }
+          *reinterpret_cast<float4 *>(col + z) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+      } else {
+#pragma unroll
+        for (int z = 0; z < SP_TZ; z++) {
+          float lo, hi;
+          unpack2(acc[z], lo, hi);
+          if (z0 + z < K2) col[z] = c ? hi : lo;
+        }
+      }
+    }
+  } else {
+    // partial bricks to shared memory (over the staging rows), summed over the
+    // group's warps in warp order, stored with consecutive threads on
+    // consecutive z (coalesced)
+    group_sync<NS>(group);
+    float *part = reinterpret_cast<float *>(&st);  // [k * 32 + z][33]: column 2 lx + k of lane
+#pragma unroll
+    for (int z = 0; z < SP_TZ; z++) {
+      float v0, v1;
+      unpack2(acc[z], v0, v1);
+      part[z * 33 + lane] = v0;
+      part[(32 + z) * 33 + lane] = v1;
+    }
+    group_sync<NS>(group);
+    const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * NS * sp_stage_bytes<P>());
+    const size_t mstride = sp_stage_bytes<P>() / sizeof(float);
+    for (int p = gt; p < SP_TX * SP_TY * SP_TZ; p += gn) {
+      const int z = p & 31, col = p >> 5;
+      const int xr = col >> 3, yr = col & 7;
+      const int src = ((xr & 1) * 32 + z) * 33 + (xr >> 1) + 4 * yr;
+      float v = gpart[src];
+#pragma unroll
+      for (int m = 1; m < NS; m++) v += gpart[m * mstride + src];
+      const int gx = x0 + xr, gy = y0 + yr, gz = z0 + z;
+      if (gx < K0 && gy < K1 && gz < K2) A.grid[((long)gx * K1 + gy) * K2 + gz] = v;
+    }
   }
 }
 
@@ -343,9 +403,13 @@ static int sm_count() {
 
 int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
                   const float4 *rec_sorted, float *grid, cudaStream_t st) {
+  static_assert(kSpreadZShift == 5, "the spread's bricks are 32 cells deep, one bucket");
   SpArgs A{};
   A.g = g;
   A.cs = cell_start;
+  const long nb = sort_buckets(g, kSpreadZShift);
+  A.head = reinterpret_cast<const uint32_t *>(cell_start) + nb + 3;  // layout of cell_count_words
+  A.tail = A.head + nb;
   A.keys = keys_sorted;
   A.rec = rec_sorted;
   A.grid = grid;
@@ -353,12 +417,11 @@ int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const u
   A.nty = (g.K1 + SP_TY - 1) / SP_TY;
   A.ntz = (g.K2 + SP_TZ - 1) / SP_TZ;
   A.nbricks = A.ntx * A.nty * A.ntz;
-  A.zshift = kSpreadZShift;
   A.nzb = (g.K2 + (1 << kSpreadZShift) - 1) >> kSpreadZShift;
   A.K2d = FastDiv((uint32_t)g.K2);
   // Split a brick's atoms over more warps while the bricks alone would not
-  // fill the SMs (4 CTAs of 4 warps resident per SM).
-  const long want = (long)sm_count() * 16;
+  // fill the SMs (5 CTAs of 4 warps resident per SM).
+  const long want = (long)sm_count() * 20;
   int nsplit = 1;
   while (nsplit < SP_WARPS && (long)A.nbricks * nsplit < want) nsplit *= 2;
   switch (g.order) {
