@@ -632,6 +632,62 @@ def run_profile(args):
                       "energy": float(ev[0].item())}), flush=True)
 
 
+def run_cufft_compare(args):
+    """`--cufft-compare`: the solve's own FFT stages (fft_forward = z/y r2c
+    passes, fft_inverse = y/z c2r passes, CUDA events per stage, L2 flushed)
+    beside cuFFT's full 3-D FP32 r2c and c2r of the same grid (torch.fft, a
+    cross-check only: nothing in the library calls cuFFT).  Prints one JSON
+    line; the x pass of this library is fused with the convolution, so the
+    fair sum is fft_forward + convolution + fft_inverse against
+    cuFFT r2c + c2r."""
+    import torch
+
+    from ewaldcorrel_b200.device import SpmeSolver
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    c = load_workload(args.workload)
+    stream = torch.cuda.Stream(dev)
+    solver = SpmeSolver(c.L, c.K, c.order, c.beta, c.max_m, device=0, stream=stream)
+    x = torch.from_numpy(c.x).to(dev)
+    q = torch.from_numpy(c.q).to(dev)
+    dx = torch.empty((c.n, 3), dtype=torch.float64, device=dev)
+    phi = torch.empty(c.n, dtype=torch.float64, device=dev)
+    ev = torch.empty(7, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    ours = {}
+    for i in range(8):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        st = solver.solve_timed(x, q, dx, phi, ev)
+        if i >= 3:
+            for k_, v in st.items():
+                ours.setdefault(k_, []).append(v)
+    ours = {k_: statistics.median(v) for k_, v in ours.items()}
+    g = torch.randn(c.K, dtype=torch.float32, device=dev)
+    cu = {"r2c": [], "c2r": []}
+    for i in range(8):
+        flush.zero_()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        F = torch.fft.rfftn(g)
+        e1.record()
+        torch.fft.irfftn(F, s=c.K)
+        e2.record()
+        torch.cuda.synchronize(dev)
+        if i >= 3:
+            cu["r2c"].append(e0.elapsed_time(e1))
+            cu["c2r"].append(e1.elapsed_time(e2))
+    cu = {k_: statistics.median(v) for k_, v in cu.items()}
+    print(json.dumps({"cufft_compare": args.workload, "grid": list(c.K),
+                      "ours_ms": {k_: ours[k_] for k_ in ("fft_forward", "convolution", "fft_inverse")},
+                      "ours_fft_conv_total_ms": ours["fft_forward"] + ours["convolution"] + ours["fft_inverse"],
+                      "cufft_ms": cu, "cufft_total_ms": cu["r2c"] + cu["c2r"],
+                      "note": "ours: z/y r2c passes; x pass + Ewald convolution + energy/virial + inverse x pass; "
+                              "y/z c2r passes (FP32, deconvolution included). cuFFT: plain 3-D FP32 r2c and c2r"}),
+          flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -640,11 +696,16 @@ def main(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--cufft-compare", action="store_true",
+                    help="time the solve's FFT stages beside cuFFT on the same grid and exit (no timing line)")
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="run this many plain solves for a profiler capture and exit (no timing line)")
     args = ap.parse_args(argv)
     if args.profile_solves > 0:
         run_profile(args)
+        return
+    if args.cufft_compare:
+        run_cufft_compare(args)
         return
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
