@@ -30,6 +30,7 @@ struct Handle {
   SplineNodes nodes{};
   int state = -1;  // -1: nothing computed, 0: structure factor, 1: potential grid
   int a_mode = 0;  // 0: no influence function, 1: host tables, 2: Ewald on device, 3: sampled radial function
+  int ewald_src = 0;  // sfac_set_ewald: 0 pick by grid size, 2 always evaluate on the device (no table)
   Influence inf{};
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is enqueued on
@@ -914,6 +915,7 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   const size_t nm = (size_t)h->nmodes;
   bool table = 56 * nm <= kEwaldTableMaxBytes;
   bool compact = !table;
+  if (h->ewald_src == 2) table = compact = false;  // the box may change on the device (sfac_box_update_device)
   if (const char *e = getenv("SFAC_EWALD_TABLE")) {
     if (e[0] == '0' && e[1] == 0) table = compact = false;  // evaluate the images in every solve
     if (e[0] == 'c' && e[1] == 0) table = !(compact = true);  // compact table whatever the size
@@ -939,6 +941,38 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   h->inf = inf;
   h->a_mode = 2;
   return 0;
+}
+
+// Box constants from a box L = [ax, by, cz, bx, cx, cy] in device memory,
+// with make_cell's expressions and operation order (explicit round-to-nearest
+// operations, no contraction: the same bits as the host's Cell), and the
+// device Ewald constants of that box (beta, max_m, fac fixed by the handle).
+__global__ void box_from_device_kernel(const double *__restrict__ L, CellConst *cell, InfConst *ic, double beta,
+                                       double max_m, double fac) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double L0 = L[0], L1 = L[1], L2 = L[2], L3 = L[3], L4 = L[4], L5 = L[5];
+  CellConst c{};
+  c.iV = __ddiv_rn(1.0, __dmul_rn(__dmul_rn(L0, L1), L2));
+  c.iL00 = __ddiv_rn(1.0, L0);
+  c.iL11 = __ddiv_rn(1.0, L1);
+  c.iL22 = __ddiv_rn(1.0, L2);
+  c.iL10 = __dmul_rn(__dmul_rn(-L3, L2), c.iV);
+  c.iL20 = __dmul_rn(__dsub_rn(__dmul_rn(L3, L5), __dmul_rn(L1, L4)), c.iV);
+  c.iL21 = __dmul_rn(__dmul_rn(-L0, L5), c.iV);
+  *cell = c;
+  *ic = InfConst{c.iL00, c.iL10, c.iL11, c.iL20, c.iL21, c.iL22, beta, max_m, fac};
+}
+
+int sfac_box_update_device(void *p, const double *L_dev) {
+  Handle *h = H(p);
+  if (!h || !L_dev) return 1;
+  if (h->a_mode != 2 || h->inf.mode != 2) {
+    printf("sfac_box_update_device: needs sfac_set_ewald with SFAC_TUNE_EWALD_SOURCE = 2\n");
+    return 1;
+  }
+  box_from_device_kernel<<<1, 32, 0, h->stream>>>(L_dev, h->d_cell, h->d_ic, h->hic.beta, h->hic.max_m, h->hic.fac);
+  const int k = 1 + launch_ewald_rows(h->geom, h->inf, h->d_rows, h->stream);
+  return launched(h, k, "box update") ? 0 : 2;
 }
 
 int sfac_set_stream(void *p, void *stream) {
@@ -1067,6 +1101,11 @@ int sfac_set_tuning(void *p, int key, int value) {
     if (value < 0 || value > 64 || (value & (value - 1))) return 1;
     h->fft.x_lines = value;
     h->version++;
+    return 0;
+  }
+  if (key == SFAC_TUNE_EWALD_SOURCE) {
+    if (value != 0 && value != 2) return 1;
+    h->ewald_src = value;
     return 0;
   }
   if (key == SFAC_TUNE_ZY_MODE) {

@@ -2,17 +2,19 @@
 
 ``SpmeServer`` wraps the native serving runtime of libsfac.so
 (``spme_server_*`` in include/sfac.h): a persistent pool of solver slots with
-resident grids, moduli, twiddles and influence tables, admission by device
-memory footprint, one stream per slot so that admitted requests overlap on the
-GPU, and CUDA-graph replay of every slot's solve.
+resident grids, moduli and twiddles, admission by device memory footprint,
+one stream per slot so that admitted requests overlap on the GPU, and one
+captured CUDA graph per slot that takes each request's box on the device.
 
-``run_stream`` drives it with timed arrivals: requests are submitted as soon
-as they have arrived and a slot (or memory for a new one) is free, completions
-are polled, and per-request latency (arrival to completion) is recorded.
-``autotune`` picks, per (grid, order) shape, the x-FFT lines per CTA from
-per-stage CUDA-event timings.  ``run_plain`` is the baseline: one request at
-a time, its kernels launched one by one (no graph), waited for before the
-next request.
+``SpmeServer.run_stream_native`` serves a whole request stream in native code
+(each request's positions and charges are copied in from the caller's memory
+with the request; the serving loop submits, polls and records latency from
+arrival to completion).
+``run_stream`` drives the same server from Python, request by request, and
+can keep outputs (the tests use it).  ``run_plain`` is the baseline: the plain
+one-solve-per-launch path -- one request at a time through the same runner
+and graphs, each waited for before the next.  ``autotune`` picks, per (grid,
+order) shape, the x-FFT lines per CTA from per-stage CUDA-event timings.
 """
 from __future__ import annotations
 
@@ -45,8 +47,12 @@ def _lib():
         lib.spme_server_poll.restype = c_int
         lib.spme_server_tune.argtypes = [c_void_p, _int3, c_int, c_int]
         lib.spme_server_tune.restype = c_int
+        lib.spme_server_set_work_budget.argtypes = [c_void_p, c_double]
+        lib.spme_server_set_work_budget.restype = c_int
         lib.spme_server_stats.argtypes = [c_void_p, POINTER(c_double)]
         lib.spme_server_stats.restype = c_int
+        lib.spme_server_run_stream.argtypes = [c_void_p, c_int] + [c_void_p] * 9 + [c_void_p, c_void_p, c_void_p]
+        lib.spme_server_run_stream.restype = c_int
         lib.sfac_set_tuning.argtypes = [c_void_p, c_int, c_int]
         lib.sfac_set_tuning.restype = c_int
         lib.sfac_solve_device_timed.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [POINTER(c_float)]
@@ -103,6 +109,35 @@ class SpmeServer:
         buffer holds the results, 2 that the request's GPU work failed."""
         k = self.lib.spme_server_poll(self.h, self._ids, self._status, 1024)
         return [(self._ids[i], self._status[i]) for i in range(k)]
+
+    def run_stream_native(self, specs, arrivals, pool, qpool):
+        """Serves the request stream `specs` (cfg5-style dicts: n, side, K,
+        order, beta, max_m; request i sends the fractional positions
+        pool[:n] of its cubic box of side `side` and charges qpool[:n])
+        arriving at `arrivals` seconds (None: all at once) entirely in native
+        code (spme_server_run_stream).  Returns (latencies in s, wall s)."""
+        m = len(specs)
+        n = np.ascontiguousarray([sp["n"] for sp in specs], dtype=np.int32)
+        K = np.ascontiguousarray([sp["K"] for sp in specs], dtype=np.int32).reshape(-1)
+        order = np.ascontiguousarray([sp["order"] for sp in specs], dtype=np.int32)
+        beta = np.ascontiguousarray([sp["beta"] for sp in specs], dtype=np.float64)
+        max_m = np.ascontiguousarray([sp["max_m"] for sp in specs], dtype=np.float64)
+        side = np.ascontiguousarray([sp["side"] for sp in specs], dtype=np.float64)
+        arr = np.zeros(m) if arrivals is None else np.ascontiguousarray(arrivals, dtype=np.float64)
+        lat = np.zeros(m)
+        wall = np.zeros(1)
+        self.loop_stats = np.zeros(4)
+        rc = self.lib.spme_server_run_stream(self.h, m, *(a.ctypes.data for a in (n, K, order, beta, max_m, side, arr,
+                                                                                   pool, qpool)),
+                                             lat.ctypes.data, wall.ctypes.data, self.loop_stats.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"spme_server_run_stream failed ({rc})")
+        return lat, float(wall[0])
+
+    def set_work_budget(self, nbytes):
+        """Admission by working set (spme_server_set_work_budget)."""
+        if self.lib.spme_server_set_work_budget(self.h, float(nbytes)) != 0:
+            raise ValueError("bad work budget")
 
     def tune(self, K, order, x_lines):
         self.lib.spme_server_tune(self.h, np.asarray(K, np.int32), int(order), int(x_lines))
@@ -184,15 +219,16 @@ def run_stream(server: SpmeServer, requests, arrivals=None, make_x=None, max_inf
     return lat, time.perf_counter() - t0, outs
 
 
-def run_plain(requests, make_x=None, device=0, warm=True):
-    """Baseline: one request at a time -- copy in, launch the solve's kernels
-    one by one (no graph), copy out, wait -- with resident per-shape solvers
-    (a first pass, untimed, creates them)."""
-    server = SpmeServer(device=device, max_inflight=1, graphs=False)
+def run_plain(specs, pool, qpool, device=0, warm=True):
+    """Baseline: the plain one-solve-per-launch GPU path -- one request at a
+    time (copy in, its captured CUDA graph, copy out, wait) through the same
+    native runner, slots and graphs as the served stream, with resident
+    per-shape solvers (a first pass, untimed, creates them)."""
+    server = SpmeServer(device=device, max_inflight=1, graphs=True)
     try:
         if warm:
-            run_stream(server, requests, None, make_x, max_inflight=1)
-        lat, wall, _ = run_stream(server, requests, None, make_x, max_inflight=1)
+            server.run_stream_native(specs, None, pool, qpool)
+        lat, wall = server.run_stream_native(specs, None, pool, qpool)
     finally:
         server.close()
     return lat, wall
@@ -246,13 +282,14 @@ def percentiles(lat):
             "mean": float(srt.mean() * 1e3)}
 
 
-def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, device=0, tune=True,
+def stream_benchmark(count=10000, plain_count=2000, load=0.8, max_inflight=64, device=0, tune=False,
                      budget_bytes=48 << 30, seed=5):
     """The serving-stream measurement: `count` requests (cfg5 shapes: 500 to
-    200,000 atoms, 24^3 to 128^3 grids, order 4 or 6), served with
-    continuous batching; capacity from a closed-loop pass, then Poisson
-    arrivals at `load` x capacity for latency; the plain path on the first
-    `plain_count` requests.  Returns a dict of results."""
+    200,000 atoms, 24^3 to 128^3 grids, order 4 or 6) served natively with
+    continuous admission (spme_server_run_stream); capacity from a
+    closed-loop pass, then Poisson arrivals at `load` x capacity for latency;
+    the plain one-at-a-time path on the first `plain_count` requests.
+    Returns a dict of results."""
     import collections
 
     import torch
@@ -260,21 +297,17 @@ def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, d
     from . import configs
 
     specs = configs.cfg5_specs(count, seed)
-    pool = configs.cfg5_pool(seed)
+    pool = _pinned((configs.CFG5_POOL_ATOMS, 3))
+    pool[:] = configs.cfg5_pool(seed)
     qpool = _pinned(configs.CFG5_POOL_ATOMS)
     qpool[:] = configs.cfg5_charges(configs.CFG5_POOL_ATOMS)
-    reqs = [Request(s["id"], None, qpool[: s["n"]], [s["side"], s["side"], s["side"], 0, 0, 0], s["K"], s["order"],
-                    s["beta"], s["max_m"]) for s in specs]
-
-    def make_x(r, buf):
-        np.multiply(pool[: r.n], r.L[0], out=buf[: r.n])
 
     tunes = {}
     t_tune = time.perf_counter()
     if tune:
         by_shape = collections.defaultdict(list)
-        for r in reqs:
-            by_shape[(tuple(int(k) for k in r.K), r.order)].append(r.n)
+        for sp in specs:
+            by_shape[(tuple(int(k) for k in sp["K"]), sp["order"])].append(sp["n"])
         shapes = [(K, o, int(np.median(ns))) for (K, o), ns in sorted(by_shape.items())]
         tunes = autotune(shapes, device=device)
     t_tune = time.perf_counter() - t_tune
@@ -283,17 +316,25 @@ def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, d
     for (K, o), xl in tunes.items():
         srv.tune(K, o, xl)
     torch.cuda.synchronize(device)
-    _, t_warm, _ = run_stream(srv, reqs, None, make_x, max_inflight=max_inflight)  # slots + graphs
-    _, t_cap, _ = run_stream(srv, reqs, None, make_x, max_inflight=max_inflight)
+    # warm until a pass creates no slot: every shape the stream needs at its
+    # concurrency is resident (grids, plans, graphs), as in steady serving
+    t_warm = 0.0
+    for _ in range(6):
+        c0 = srv.stats()["created"]
+        _, t = srv.run_stream_native(specs, None, pool, qpool)
+        t_warm += t
+        if srv.stats()["created"] == c0:
+            break
+    _, t_cap = srv.run_stream_native(specs, None, pool, qpool)
     capacity = count / t_cap
     rng = np.random.default_rng(seed)
     arrivals = np.cumsum(rng.exponential(1.0 / (load * capacity), size=count))
-    lat, t_open, _ = run_stream(srv, reqs, arrivals, make_x, max_inflight=max_inflight)
+    lat, t_open = srv.run_stream_native(specs, arrivals, pool, qpool)
     stats = srv.stats()
     srv.close()
 
-    sample = reqs[:plain_count]
-    plat, t_plain = run_plain(sample, make_x, device=device)
+    sample = specs[:plain_count]
+    plat, t_plain = run_plain(sample, pool, qpool, device=device)
     plain = len(sample) / t_plain
     return {
         "requests": count,
@@ -311,7 +352,8 @@ def stream_benchmark(count=10000, plain_count=1000, load=0.8, max_inflight=48, d
         "warm_pass_s": t_warm,
         "autotune_s": t_tune,
         "autotuned_shapes": len(tunes),
-        "mean_atoms": float(np.mean([r.n for r in reqs])),
+        "mean_atoms": float(np.mean([sp["n"] for sp in specs])),
+        "plain": "one request at a time through the same runner: copy in, captured CUDA graph, copy out, wait",
     }
 
 
@@ -322,13 +364,15 @@ def main(argv=None):
     import json
 
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--count", type=int, default=3000)
-    ap.add_argument("--plain", type=int, default=1000)
+    ap.add_argument("--count", type=int, default=10000)
+    ap.add_argument("--plain", type=int, default=2000)
     ap.add_argument("--load", type=float, default=0.8)
-    ap.add_argument("--max-inflight", type=int, default=48)
+    ap.add_argument("--max-inflight", type=int, default=64)
+    ap.add_argument("--tune", action="store_true")
     args = ap.parse_args(argv)
     t0 = time.perf_counter()
-    res = stream_benchmark(count=args.count, plain_count=args.plain, load=args.load, max_inflight=args.max_inflight)
+    res = stream_benchmark(count=args.count, plain_count=args.plain, load=args.load, max_inflight=args.max_inflight,
+                           tune=args.tune)
     res["wall_s"] = time.perf_counter() - t0
     print(json.dumps(res))
 

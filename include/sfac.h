@@ -207,17 +207,34 @@ int sfac_solve_device_timed(void *sfac, int n, const double *x, const double *w,
 int sfac_cell_sort_noalloc(const double L[6], const int K[3], int n, const double *x, int *keys, int *perm,
                            void *stream);
 
+/* Replaces the box from DEVICE memory: L_dev (6 doubles on the handle's
+ * device, [ax, by, cz, bx, cx, cy]) is read when the enqueued work runs, so a
+ * captured CUDA graph can take a new box with each replay.  Updates the
+ * device box constants (the same bits as set_L would give) and rebuilds the
+ * Ewald row tables; the device solves that follow use the new box.  Needs
+ * sfac_set_ewald under SFAC_TUNE_EWALD_SOURCE = 2 (influence evaluated per
+ * solve, no table to rebuild).  The host-side calls (sfac, en, de1, de2,
+ * potl, sfac_real_space) keep the box last set on the host.  Enqueued on the
+ * handle's stream without synchronising.  Returns 0, 1 (wrong influence
+ * source), 2 (CUDA error).  No counterpart in the reference. */
+int sfac_box_update_device(void *sfac, const double *L_dev);
+
 /* Use (1) or bypass (0) CUDA-graph replay in sfac_solve_device*.
  * Returns 0. */
 int sfac_set_graphs(void *sfac, int enable);
 
 /* Tuning knobs chosen by an autotuner (0 restores the heuristic):
  * SFAC_TUNE_X_LINES: x-FFT lines per CTA (power of two, <= 64).
+ * SFAC_TUNE_EWALD_SOURCE: 0 (default) lets sfac_set_ewald tabulate the
+ *   influence function when the table stays in L2; 2 always evaluates it on
+ *   the device per solve (needed by sfac_box_update_device).  Takes effect at
+ *   the next sfac_set_ewald.
  * SFAC_TUNE_ZY_MODE: z/y FFT passes: 1 fused x-plane kernels (when a plane
  *   fits in shared memory), 2 two-level register passes, 3 Stockham passes.
  * Returns 0, or 1 for an unknown key or bad value. */
 #define SFAC_TUNE_X_LINES 1
 #define SFAC_TUNE_ZY_MODE 2
+#define SFAC_TUNE_EWALD_SOURCE 3
 int sfac_set_tuning(void *sfac, int key, int value);
 
 /* Estimated device + pinned-host bytes of a handle with grid K solving n
@@ -226,30 +243,61 @@ unsigned long sfac_footprint_bytes(const int K[3], int n);
 
 /* ---- serving runtime (server.cu) ----------------------------------------
  * A persistent solver pool on one GPU.  Requests (host FP64 arrays) are
- * admitted into slots -- one handle with resident grids, moduli, twiddles
- * and fixed buffers per (grid, order, Ewald parameters, atom-count bucket)
- * -- while the pool's device-memory budget allows (idle slots are evicted
+ * admitted into slots -- one handle with resident grids, moduli and twiddles
+ * and fixed buffers per (grid, order, Ewald parameters, atom-count bucket) --
+ * while the pool's device-memory budget allows (idle slots are evicted
  * least-recently-used first); each slot runs on its own stream, so requests
- * overlap on the GPU, and replays its solve as a CUDA graph.  Atoms are
- * padded to the bucket size with zero charges (no effect on results).
- * spme_server_submit copies nothing synchronously when x, q and out are
- * pinned; out receives [E, vir(6), dE/dx (3n), phi (n)] once
- * spme_server_poll has reported the request id.  Returns of submit: 0
+ * overlap on the GPU.  Each request's box may differ: the slot takes it on
+ * the device (sfac_box_update_device), so one captured CUDA graph per slot
+ * serves every request: copy in, graph launch, copy out, event.  Atoms are
+ * padded to the bucket size with zero charges (no effect on results).  out
+ * receives [E, vir(6), dE/dx (3n), phi (n)] once spme_server_poll has
+ * reported the request id; the host arrays must stay untouched until then
+ * (pinned memory makes the copies asynchronous).  Returns of submit: 0
  * admitted, 1 no slot or memory free now (poll, then retry), 2 error.
- * Not thread-safe: one host thread drives a server. */
+ * Not thread-safe: one host thread drives a server.  No counterpart in the
+ * reference (its library solves one system per handle). */
 void *spme_server_create(int device, double budget_bytes, int max_inflight, int use_graphs);
 void spme_server_destroy(void *server);
 int spme_server_submit(void *server, long long id, int n, const int K[3], int order, double beta, double max_m,
                        const double L[6], const double *x, const double *q, double *out);
+/* The same request as one packed host block of 16 + 4n doubles:
+ * [L(6), n, f, 8 unused | x (3n) | q (n)], f = 1 when x holds fractional
+ * coordinates of the box (else 0); one copy in instead of three. */
+int spme_server_submit_packed(void *server, long long id, int n, const int K[3], int order, double beta,
+                              double max_m, const double *block, double *out);
 /* Completed requests: up to max_ids ids, each with its status (0: out holds
  * the results; 2: the request's GPU work failed and out is not valid).
  * status may be NULL.  Returns the number of ids written. */
 int spme_server_poll(void *server, long long *ids, int *status, int max_ids);
-/* Sets x-FFT lines per CTA for slots of grid K and order (autotuner result). */
+/* Admission by working set: a request waits (submit returns 1) while the
+ * requests in flight plus it would hold more than `bytes` of grids and atom
+ * buffers, unless nothing is in flight.  Concurrent solves whose working
+ * sets outgrow the L2 cache all run slower; the default is 256 MB. */
+int spme_server_set_work_budget(void *server, double bytes);
+/* Sets x-FFT lines per CTA for slots of grid K and order created from now on
+ * (autotuner result). */
 int spme_server_tune(void *server, const int K[3], int order, int x_lines);
 /* stats[0..7] = slots, bytes in use, solves, slots created, slots evicted,
  * errors, in flight, budget. */
 int spme_server_stats(void *server, double *stats);
+/* A whole request stream, served natively (the serving benchmark): request
+ * i (ids 0..nreq-1, in arrival order) has n[i] atoms in a cubic box of side
+ * side[i], its positions given as fractional coordinates frac_pool[0 ..
+ * 3 n[i]) (copied in with the request and turned into x = s * side on the
+ * device) and its charges q_pool[0 .. n[i]), grid K[3i..3i+2], order[i],
+ * beta[i], max_m[i]; it arrives at arrival[i] seconds after the start (0: all
+ * at once).  The loop submits in arrival order within the server's
+ * in-flight limit and work budget (a request that does not fit the budget
+ * yet is passed by later arrived ones that do, up to 64 waiting), polls,
+ * and stores latency[i] = completion -
+ * arrival (seconds) and the wall time.  frac_pool and q_pool should be
+ * pinned.  loop_stats (4 doubles, may be NULL): seconds the loop spent in
+ * submissions and in polls, submissions tried, polls.  Returns 0, 1 bad
+ * arguments, 2 failure. */
+int spme_server_run_stream(void *server, int nreq, const int *n, const int *K, const int *order, const double *beta,
+                           const double *max_m, const double *side, const double *arrival, const double *frac_pool,
+                           const double *q_pool, double *latency, double *wall, double *loop_stats);
 
 /* Debug views (copies to host; for parity tests).
  * sfac_debug_sort: cell keys and original indices in sorted order (n each)

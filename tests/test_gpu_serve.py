@@ -99,3 +99,78 @@ def test_small_budget_evicts_and_stays_correct():
     assert st["evicted"] > 0 and st["bytes"] <= budget and st["errors"] == 0
     for r in reqs:
         _compare(out[r.id], ref[r.id], f"request {r.id}")
+
+
+def test_packed_submit_matches_oracle():
+    """spme_server_submit_packed (one packed block [box, n, f | x | q]) gives
+    the oracle's results, on slots whose box changes on the device between
+    requests of the same shape, with Cartesian and with fractional (f = 1)
+    positions."""
+    import ctypes
+
+    from ewaldcorrel_b200.serve import SpmeServer, _lib, _pinned
+    from oracle.oracle import OracleSfac
+
+    lib = _lib()
+    lib.spme_server_submit_packed.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                              ctypes.c_void_p]
+    lib.spme_server_submit_packed.restype = ctypes.c_int
+    rng = np.random.default_rng(3)
+    srv = SpmeServer(max_inflight=4)
+    K = np.array([32, 32, 32], np.int32)
+    cases = []
+    for i, side in enumerate((3.0, 3.3, 2.8)):  # same shape, new box each time
+        n = 1200
+        frac = i == 2  # the last one sends fractional coordinates (flag word 7)
+        s = rng.uniform(0, 1, size=(n, 3))
+        x = s * side
+        q = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+        blk = _pinned(16 + 4 * n)
+        blk[:] = 0.0
+        blk[0:3] = side
+        blk[6] = n
+        blk[7] = 1.0 if frac else 0.0
+        blk[16:16 + 3 * n] = (s if frac else x).ravel()
+        blk[16 + 3 * n:] = q
+        out = _pinned(7 + 4 * n)
+        rc = lib.spme_server_submit_packed(srv.h, i, n, K.ctypes.data, 4, 3.12, 6.0, blk.ctypes.data, out.ctypes.data)
+        assert rc == 0
+        done = []
+        while not done:
+            done = srv.poll()
+        assert done == [(i, 0)]
+        cases.append((side, x, q, out.copy()))
+    srv.close()
+    for side, x, q, out in cases:
+        n = len(q)
+        o = OracleSfac(np.array([side, side, side, 0, 0, 0]), K, 4)
+        o.set_ewald(3.12, 6.0)
+        o.sfac(q, x)
+        vir = np.zeros(6)
+        e = o.de1(vir)
+        dx = np.zeros((n, 3))
+        phi = np.zeros(n)
+        o.de2(n, q, x, dx)
+        o.potl(n, x, phi)
+        _compare((out[0], out[1:7], out[7:7 + 3 * n].reshape(n, 3), out[7 + 3 * n:]), (e, vir, dx, phi),
+                 f"box {side}")
+
+
+def test_native_stream_runner():
+    """spme_server_run_stream serves a stream (all at once, then with timed
+    arrivals) with no errors and a latency for every request."""
+    from ewaldcorrel_b200.serve import SpmeServer
+
+    specs = [s for s in configs.cfg5_specs(400) if s["n"] <= 40000][:60]
+    pool = configs.cfg5_pool()
+    qpool = configs.cfg5_charges(configs.CFG5_POOL_ATOMS)
+    srv = SpmeServer(max_inflight=16)
+    lat, wall = srv.run_stream_native(specs, None, pool, qpool)
+    assert wall > 0 and np.all(lat > 0)
+    arrivals = np.cumsum(np.full(len(specs), 100e-6))
+    lat, wall = srv.run_stream_native(specs, arrivals, pool, qpool)
+    st = srv.stats()
+    srv.close()
+    assert np.all(lat > 0) and wall >= arrivals[-1]
+    assert st["errors"] == 0 and st["solves"] == 2 * len(specs)
