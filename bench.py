@@ -523,6 +523,25 @@ def run_b200(args, rank, world, local_rank):
             "potential_rel_rms": float(np.sqrt(np.mean((phig - phi_ref) ** 2) / np.mean(phi_ref ** 2))),
             "virial_max_rel": float(np.abs(ev_host[1:] - vir_ref).max() / np.abs(vir_ref).max()),
         }
+    if world == 1 and not args.no_serving:
+        # the serving stream beside the solve (10,000 requests of the
+        # serving workload, 500 to 200,000 atoms, 24^3 to 128^3, order 4/6):
+        # served (continuous admission) vs the plain one-at-a-time path
+        from ewaldcorrel_b200 import serve
+
+        sv = serve.stream_benchmark(count=10000, plain_count=2000, device=local_rank)
+        line["serving"] = {
+            "workload": "10,000 requests: atoms log-uniform in [500, 200000], cubic boxes at 100 atoms/nm^3, "
+                        "grids 24^3..128^3 (2/3/5-smooth, 0.1 nm), order 4 or 6, beta 3.12; Poisson arrivals at "
+                        f"{sv['offered_load']:.0%} of capacity",
+            "served_over_plain": sv["served_over_plain"],
+            "capacity_solves_per_s": sv["capacity_solves_per_s"],
+            "served_solves_per_s": sv["served_solves_per_s"],
+            "latency_ms": sv["latency_ms"],
+            "plain_solves_per_s": sv["plain_solves_per_s"],
+            "plain": sv["plain"],
+            "errors": sv["errors"],
+        }
     line["clocks"] = clocks
     if dist is not None:
         dist.barrier()
@@ -695,6 +714,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--cufft-compare", action="store_true",
                     help="time the solve's FFT stages beside cuFFT on the same grid and exit (no timing line)")

@@ -26,7 +26,7 @@
 #include <vector>
 
 #include "../../include/sfac.h"
-#include "spme_common.cuh"
+#include "spme_kernels.hpp"
 
 namespace {
 
@@ -189,11 +189,11 @@ Slot *create_slot(Server *sv, int ncap, const int K[3], int order, double beta, 
     if (ok && t.K[0] == K[0] && t.K[1] == K[1] && t.K[2] == K[2] && t.order == order)
       sfac_set_tuning(s->h, SFAC_TUNE_X_LINES, t.x_lines);
   const size_t nb = kHdr + 4 * (size_t)ncap;
-  ok = ok && cudaMalloc((void **)&s->d_blk, sizeof(double) * nb) == cudaSuccess &&
-       cudaMalloc((void **)&s->d_x, sizeof(double) * 3 * ncap) == cudaSuccess &&
-       cudaMalloc((void **)&s->d_q, sizeof(double) * ncap) == cudaSuccess &&
-       cudaMalloc((void **)&s->d_phi, sizeof(double) * ncap) == cudaSuccess &&
-       cudaMalloc((void **)&s->d_out, sizeof(double) * (8 + 4 * (size_t)ncap)) == cudaSuccess &&
+  ok = ok && spme::device_malloc((void **)&s->d_blk, sizeof(double) * nb) == cudaSuccess &&
+       spme::device_malloc((void **)&s->d_x, sizeof(double) * 3 * ncap) == cudaSuccess &&
+       spme::device_malloc((void **)&s->d_q, sizeof(double) * ncap) == cudaSuccess &&
+       spme::device_malloc((void **)&s->d_phi, sizeof(double) * ncap) == cudaSuccess &&
+       spme::device_malloc((void **)&s->d_out, sizeof(double) * (8 + 4 * (size_t)ncap)) == cudaSuccess &&
        cudaMallocHost((void **)&s->h_blk, sizeof(double) * nb) == cudaSuccess &&
        cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming) == cudaSuccess;
   if (ok && write_value32()) {  // completion word (events remain the fallback)

@@ -3,6 +3,7 @@
 // the state machine follow sfac.cpp; every computation on grids or atoms runs
 // on the GPU.  No C++ exception crosses the C ABI: failures return NULL/0 and
 // are recorded in the handle (sfac_last_error).
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -10,10 +11,40 @@
 #include <new>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sfac.h"
 #include "spme_kernels.hpp"
 
 using namespace spme;
+
+namespace {
+// NVTX range over a scope: names each stage and C-API call on a profiler's
+// timeline (header-only NVTX; nearly free when no tool is attached).
+struct Nvtx {
+  explicit Nvtx(const char *name) { nvtxRangePushA(name); }
+  ~Nvtx() { nvtxRangePop(); }
+};
+}  // namespace
+
+namespace spme {
+
+// > 0: the fail_alloc_in-th device allocation from now on fails (and the
+// counter stops); 0: allocations go straight to cudaMalloc.
+static std::atomic<int> fail_alloc_in{0};
+
+cudaError_t device_malloc(void **p, size_t bytes) {
+  int k = fail_alloc_in.load();
+  while (k > 0 && !fail_alloc_in.compare_exchange_weak(k, k - 1)) {
+  }
+  if (k == 1) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+}  // namespace spme
 
 namespace {
 
@@ -132,7 +163,7 @@ bool launched(Handle *h, int n, const char *what) {
 template <class T>
 bool dalloc(Handle *h, T **p, size_t count) {
   *p = nullptr;
-  return CK(h, cudaMalloc((void **)p, sizeof(T) * (count ? count : 1)));
+  return CK(h, device_malloc((void **)p, sizeof(T) * (count ? count : 1)));
 }
 template <class T>
 void dfree(T *&p) {
@@ -425,6 +456,7 @@ void *sfac_ctor(double L[6], int K[3], int order) {
 void sfac_dtor(void *p) { destroy(H(p)); }
 
 void sfac(void *p, int n, const double *w, const double *x) {
+  Nvtx range("sfac sfac");
   Handle *h = H(p);
   if (!h) return;
   if (n < 0) {
@@ -487,6 +519,7 @@ void set_L(void *p, double L[6]) {
 // f(m^2)/2 to A and f'(m^2) m_a m_b to dA.  f runs on the host (it may be a
 // Python callable); the tables are then uploaded as FP64.
 int set_A(void *p, rad_fn f, double max_m, void *info) {
+  Nvtx range("sfac set_A");
   Handle *h = H(p);
   if (!h) return 2;
   const int K0 = h->K[0], K1 = h->K[1], K2 = h->K[2], ldim = h->ldim;
@@ -548,6 +581,7 @@ int set_A(void *p, rad_fn f, double max_m, void *info) {
 }
 
 double en(void *p) {
+  Nvtx range("sfac en");
   Handle *h = H(p);
   if (!h) return 0.0;
   if (h->state != 0) {
@@ -568,6 +602,7 @@ double en(void *p) {
 }
 
 double de1(void *p, double vir[6]) {
+  Nvtx range("sfac de1");
   Handle *h = H(p);
   if (!h) return 0.0;
   if (h->state != 0) {
@@ -623,6 +658,7 @@ static bool ensure_pipeline(Handle *h) {
 // (s_in), gather (the handle's stream) and copy out (s_out) overlap the
 // neighbouring chunks', so the two PCIe directions and the gather run at once.
 static void gather_call(Handle *h, int n, const double *w, const double *x, double *dx, double *phi) {
+  Nvtx range(dx ? "sfac de2" : "sfac potl");
   if (h->state != 1) {
     printf("Error: You must call de1 before this routine.\n");
     return;
@@ -993,17 +1029,34 @@ static int enqueue_solve(Handle *h, int n, const double *x, const double *w, dou
   cudaStream_t st = h->stream;
   int k = 0;
   if (timed) CK(h, cudaEventRecord(h->ev_stage[0], st));
-  k += launch_cell_sort(h->geom, n, x, w, h->sb, st, kSpreadZShift);
+  {
+    Nvtx r("spme cell sort");
+    k += launch_cell_sort(h->geom, n, x, w, h->sb, st, kSpreadZShift);
+  }
   if (timed) CK(h, cudaEventRecord(h->ev_stage[1], st));
-  k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real, st);
+  {
+    Nvtx r("spme spread");
+    k += launch_spread(h->geom, h->spline, h->sb.cell_start, h->sb.keys[h->sb.cur], h->sb.rec_sorted, h->d_real, st);
+  }
   if (timed) CK(h, cudaEventRecord(h->ev_stage[2], st));
   int nb = 0;
-  k += fwd_zy(h->fft, h->d_real, h->d_cplx, st);
+  {
+    Nvtx r("spme fft forward");
+    k += fwd_zy(h->fft, h->d_real, h->d_cplx, st);
+  }
   if (timed) CK(h, cudaEventRecord(h->ev_stage[3], st));
-  k += launch_x_conv(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials, nb, st);
+  {
+    Nvtx r("spme convolution");
+    k += launch_x_conv(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials, nb,
+                       st);
+  }
   if (timed) CK(h, cudaEventRecord(h->ev_stage[4], st));
-  k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->d_cell, h->d_red, ev, st);
+  {
+    Nvtx r("spme fft inverse");
+    k += inv_yz(h->fft, h->d_cplx, h->d_real, h->d_partials, nb, h->d_cell, h->d_red, ev, st);
+  }
   if (timed) CK(h, cudaEventRecord(h->ev_stage[5], st));
+  Nvtx r("spme gather");
   // gather in cell order (the sort of this solve): neighbouring threads share grid lines
   const uint32_t *perm = h->sb.vals[h->sb.cur], *skeys = h->sb.keys[h->sb.cur];
   if (dEdL)
@@ -1143,6 +1196,11 @@ int sfac_debug_sort(void *p, int n, int *keys, int *perm) {
       !CK(h, cudaMemcpyAsync(perm, h->sb.vals[h->sb.cur], sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream)))
     return 1;
   return sync(h) ? 0 : 1;
+}
+
+int sfac_debug_fail_alloc(int nth) {
+  fail_alloc_in.store(nth > 0 ? nth : 0);
+  return 0;
 }
 
 int sfac_debug_spread(void *p, float *grid) {

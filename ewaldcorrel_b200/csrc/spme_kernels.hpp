@@ -9,6 +9,11 @@
 
 namespace spme {
 
+// Every device allocation of the library (handles and the serving runtime)
+// goes through here, so that a test can make the n-th one fail
+// (sfac_debug_fail_alloc) and check the error paths without a GPU fault.
+cudaError_t device_malloc(void **p, size_t bytes);
+
 // ---- sort (k_sort.cu) ----
 struct SortBuffers {
   uint32_t *keys[2];   // [1]: cell key of every atom (input order); [0]: keys in cell order

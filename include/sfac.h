@@ -305,6 +305,12 @@ int spme_server_run_stream(void *server, int nreq, const int *n, const int *K, c
  * sfac_debug_spread: the spread grid of the last sfac call (K0*K1*K2 float),
  *   recomputed from the stored sorted atoms. */
 int sfac_debug_sort(void *sfac, int n, int *keys, int *perm);
+/* Test hook: the nth device allocation of the library from now on (handles
+ * and serving slots) fails as if the device were out of memory, once; 0
+ * disarms.  Lets tests drive the allocation-failure paths (sfac_ctor
+ * returning NULL, set_A returning 2, spme_server_submit returning 2) without
+ * exhausting a GPU.  Returns 0. */
+int sfac_debug_fail_alloc(int nth);
 int sfac_debug_spread(void *sfac, float *grid);
 
 #ifdef __cplusplus
