@@ -176,22 +176,24 @@ def algorithmic_bytes(n, K):
     }
 
 
-# DRAM bytes (read + write) per launch of each stage's kernels, from one ncu
-# capture of a plain solve (ncu --metrics dram__bytes_read.sum,
-# dram__bytes_write.sum,gpu__time_duration.sum; cold caches; summarised in
-# profiles/dram_per_kernel_water_triclinic.md).  Writes that stay in the
-# 126 MB L2 past the kernel's end are not counted by the capture.
+# DRAM bytes (read + write) per launch of each stage's kernels, from ncu
+# captures of a plain solve (cold caches; summaries in profiles/).  Writes
+# that stay in the 126 MB L2 past the kernel's end are not counted.  The
+# spread's figures are from profiles/ncu_full_spread_triclinic1m.md and
+# profiles/dram_per_kernel_water.md; the FFT and gather kernels are unchanged
+# since profiles/dram_per_kernel_water_triclinic_fft_gather.md; None: not
+# captured for the current kernels.
 NCU_TRAFFIC = {
-    "water": {"cell_sort": 24.20e6, "spread": 5.52e6, "fft_forward": 7.30e6, "convolution": 29.00e6,
-              "fft_inverse": 7.41e6, "gather": 6.70e6},
-    "triclinic": {"cell_sort": 438.63e6, "spread": 124.81e6, "fft_forward": 163.58e6, "convolution": 163.50e6,
+    "water": {"cell_sort": 7.48e6, "spread": 2.33e6, "fft_forward": 7.30e6, "convolution": 29.00e6,
+              "fft_inverse": 7.38e6, "gather": 6.70e6},
+    "triclinic": {"cell_sort": None, "spread": 43.87e6, "fft_forward": 163.58e6, "convolution": 163.50e6,
                   "fft_inverse": 165.67e6, "gather": 158.32e6},
 }
 # Kernels of each stage (the roofline is reported for the longest stage that
 # is a single kernel launch).
 STAGE_KERNELS = {
     "cell_sort": "key_count + tile_sum + cell_offsets + cell_scatter + cell_fixup (+ memset)",
-    "spread": "spread_reg_kernel",
+    "spread": "spread_kernel",
     "fft_forward": "fft_zr2c2_kernel + fft_y2_kernel<-1>",
     "convolution": "fft_x2_kernel<XM_FWD_CONV_INV> (x FFT, Ewald convolution, energy/virial, inverse x FFT)",
     "fft_inverse": "fft_y2_kernel<+1> (+ energy/virial reduction) + fft_zc2r2_kernel",
