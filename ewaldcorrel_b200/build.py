@@ -1,11 +1,16 @@
 """Builds libsfac.so (the C-ABI library with the sm_100a kernels) in-tree.
 
-    python -m ewaldcorrel_b200.build [--force] [--verbose]
+    python -m ewaldcorrel_b200.build [--force] [--verbose] [--check]
 
 nvcc cross-compiles for sm_100a without a GPU.  Objects go to
 ewaldcorrel_b200/_build/, the shared library to ewaldcorrel_b200/libsfac.so
 (next to ewald.py, which loads it from its own directory like the
 reference's wrapper does, ewald.py:52-53).
+
+--check builds the index-checking variant instead (-DSPME_CHECK: kernels
+test their indices and record the first failure in an error word rather
+than trapping): objects in _build_check/, library libsfac_check.so, loaded
+by ewald.py when EWALDCORREL_LIBSFAC names it.
 """
 from __future__ import annotations
 
@@ -20,6 +25,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libsfac.so")
+BUILD_CHECK = os.path.join(PKG, "_build_check")
+LIB_CHECK = os.path.join(PKG, "libsfac_check.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -54,18 +61,21 @@ def _mtime(p):
     return os.path.getmtime(p) if os.path.exists(p) else -1.0
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compiles every .cu under csrc/ for sm_100a and links libsfac.so."""
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, check: bool = False) -> str:
+    """Compiles every .cu under csrc/ for sm_100a and links libsfac.so
+    (libsfac_check.so with -DSPME_CHECK when check is set)."""
+    bdir, lib = (BUILD_CHECK, LIB_CHECK) if check else (BUILD, LIB)
+    extra = ["-DSPME_CHECK"] if check else []
+    os.makedirs(bdir, exist_ok=True)
     nvcc = _nvcc()
     hdr_time = max([_mtime(h) for h in _headers()] + [_mtime(__file__)])
     jobs = []
     objs = []
     for src in _sources():
-        obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if force or _mtime(obj) < max(_mtime(src), hdr_time):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-I", CSRC, "-I", INCLUDE, "-c", src, "-o", obj]
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *extra, "-I", CSRC, "-I", INCLUDE, "-c", src, "-o", obj]
             jobs.append(cmd)
 
     def run(cmd):
@@ -80,18 +90,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
-    if jobs or force or _mtime(LIB) < max(_mtime(o) for o in objs):
-        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs]
+    if jobs or force or _mtime(lib) < max(_mtime(o) for o in objs):
+        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", lib, *objs]
         run(cmd)
-    return LIB
+    return lib
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--check", action="store_true", help="index-checking build (libsfac_check.so)")
     a = ap.parse_args(argv)
-    print(build(force=a.force, verbose=a.verbose))
+    print(build(force=a.force, verbose=a.verbose, check=a.check))
 
 
 if __name__ == "__main__":

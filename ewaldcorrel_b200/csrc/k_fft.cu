@@ -18,6 +18,8 @@
 
 namespace spme {
 
+SPME_CHECK_READER(fft)
+
 // --- z pass, forward: real rows -> half-complex rows --------------------
 // CTA handles 2B real rows (B complex lines); row pitch K2 (real) / ldim.
 __global__ void __launch_bounds__(256) fft_z_r2c_kernel(FftLen L, int nrows, const float *__restrict__ rin,
@@ -414,7 +416,8 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
       float2 u[R];
 #pragma unroll
       for (int j1 = 0; j1 < R; j1++)
-        u[j1] = live ? data[line + (long)(j2 + n2 * j1) * nlines] : make_float2(0.f, 0.f);
+        u[j1] = (live && SPME_IN(j2 + n2 * j1, n, CK_FFT_LINE)) ? data[line + (long)(j2 + n2 * j1) * nlines]
+                                                                : make_float2(0.f, 0.f);
       rdft::dft<R, -1>(u);
 #pragma unroll
       for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], tw[j2 * k1]);
@@ -437,7 +440,8 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
       } else {
 #pragma unroll
         for (int k2 = 0; k2 < R; k2++)
-          w[k2] = live ? data[line + (long)(k1 + n1 * k2) * nlines] : make_float2(0.f, 0.f);
+          w[k2] = (live && SPME_IN(k1 + n1 * k2, n, CK_FFT_LINE)) ? data[line + (long)(k1 + n1 * k2) * nlines]
+                                                                  : make_float2(0.f, 0.f);
       }
       if (MODE == XM_FWD_DECONV) {
         if (live) {
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
 #pragma unroll
           for (int k2 = 0; k2 < R; k2++) {
             const int kx = k1 + n1 * k2;
-            data[line + (long)kx * nlines] = cscale(w[k2], (float)(iB0[kx] * s12));
+            if (SPME_IN(kx, n, CK_FFT_LINE)) data[line + (long)kx * nlines] = cscale(w[k2], (float)(iB0[kx] * s12));
           }
         }
       } else if (IM == 1) {
@@ -458,7 +462,9 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
 #pragma unroll
           for (int k2 = 0; k2 < R; k2++) {
             const int kx = k1 + n1 * k2;
-            const long i = ((long)kx * K1 + ky) * ldim + kz;
+            const long i = SPME_IN(((long)kx * K1 + ky) * ldim + kz, (long)n * K1 * ldim, CK_FFT_CONV)
+                               ? ((long)kx * K1 + ky) * ldim + kz
+                               : 0;
             const float2 q = w[k2];
             const double ib = iB0[kx] * s12;
             double sq = (double)q.x * q.x + (double)q.y * q.y;
@@ -497,7 +503,9 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
 #pragma unroll 1
           for (int k2 = 0; k2 < R; k2++) {
             const int kx = k1 + n1 * k2;
-            const long i = ((long)kx * K1 + ky) * ldim + kz;
+            const long i = SPME_IN(((long)kx * K1 + ky) * ldim + kz, (long)n * K1 * ldim, CK_FFT_CONV)
+                               ? ((long)kx * K1 + ky) * ldim + kz
+                               : 0;
             const float2 q = slot[k2 * B];
             const double ib = iB0[kx] * s12;
             double sq = (double)q.x * q.x + (double)q.y * q.y;
@@ -551,7 +559,8 @@ __global__ void __launch_bounds__(512) fft_x2_kernel(int n, int n1, int n2, cons
       for (int k1 = 0; k1 < R; k1++) u[k1] = ex[(k1 * n2 + j2) * B + b];
       rdft::dft<R, +1>(u);
 #pragma unroll
-      for (int j1 = 0; j1 < R; j1++) data[line + (long)(j2 + n2 * j1) * nlines] = u[j1];
+      for (int j1 = 0; j1 < R; j1++)
+        if (SPME_IN(j2 + n2 * j1, n, CK_FFT_LINE)) data[line + (long)(j2 + n2 * j1) * nlines] = u[j1];
     });
   }
 }
@@ -589,7 +598,9 @@ __global__ void __launch_bounds__(512) fft_y2_kernel(int n, int n1, int n2, cons
       constexpr int R = decltype(RI)::value;
       float2 u[R];
 #pragma unroll
-      for (int j1 = 0; j1 < R; j1++) u[j1] = live ? data[base + (long)(j2 + n2 * j1) * es] : make_float2(0.f, 0.f);
+      for (int j1 = 0; j1 < R; j1++)
+        u[j1] = (live && SPME_IN(j2 + n2 * j1, n, CK_FFT_LINE)) ? data[base + (long)(j2 + n2 * j1) * es]
+                                                                : make_float2(0.f, 0.f);
       rdft::dft<R, SIGN>(u);
 #pragma unroll
       for (int k1 = 0; k1 < R; k1++) ex[(k1 * n2 + j2) * B + b] = cmul(u[k1], twid<SIGN>(tw, j2 * k1));
@@ -605,7 +616,8 @@ __global__ void __launch_bounds__(512) fft_y2_kernel(int n, int n1, int n2, cons
       for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
       rdft::dft<R, SIGN>(w);
 #pragma unroll
-      for (int k2 = 0; k2 < R; k2++) data[base + (long)(k1 + n1 * k2) * es] = w[k2];
+      for (int k2 = 0; k2 < R; k2++)
+        if (SPME_IN(k1 + n1 * k2, n, CK_FFT_LINE)) data[base + (long)(k1 + n1 * k2) * es] = w[k2];
     });
   }
 }
@@ -710,7 +722,8 @@ __global__ void __launch_bounds__(512) fft_zr2c2_kernel(int n, int n1, int n2, c
       for (int j2 = 0; j2 < R; j2++) w[j2] = ex[(k1 * n2 + j2) * B + b];
       rdft::dft<R, -1>(w);
 #pragma unroll
-      for (int k2 = 0; k2 < R; k2++) Z[b * ZP + k1 + n1 * k2] = w[k2];
+      for (int k2 = 0; k2 < R; k2++)
+        if (SPME_IN(k1 + n1 * k2, n, CK_FFT_LINE)) Z[b * ZP + k1 + n1 * k2] = w[k2];
     });
   }
   __syncthreads();

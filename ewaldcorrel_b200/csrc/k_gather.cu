@@ -12,6 +12,8 @@
 
 namespace spme {
 
+SPME_CHECK_READER(gather)
+
 constexpr int kCellWords = 16;  // 9 used: sum_a s_a,i (dE/dr_a)_j
 
 // idx[i] = (o + i) mod K for 0 <= o < K, without a division when K >= P.
@@ -50,7 +52,9 @@ __device__ __forceinline__ void stencil_sum(const float *__restrict__ grid, cons
       float sz = 0.f, dzz = 0.f;
 #pragma unroll
       for (int k = 0; k < P; k++) {
-        const float q = __ldg(col + (WRAP ? iz[k] : k));
+        const float q = SPME_IN(col + (WRAP ? iz[k] : k) - grid, g.K0 * plane, CK_GATHER_GRID)
+                            ? __ldg(col + (WRAP ? iz[k] : k))
+                            : 0.f;
         sz = fmaf(wz[k], q, sz);
         dzz = fmaf(dwz[k], q, dzz);
       }
@@ -98,7 +102,10 @@ __global__ void __launch_bounds__(256, CELL ? 2 : 3) gather_kernel(Geom g, Splin
     float t0, t1, t2;
     if (SORTED) {
       a = (int)sv.perm[r];
-      const uint32_t key = sv.key[r];
+      uint32_t key = sv.key[r];
+      // a failed check substitutes atom 0 / key 0 (the run is flagged already)
+      if (!SPME_IN(a, n, CK_GATHER_ATOM)) a = 0;
+      if (!SPME_IN(key, (long)g.K0 * g.K1 * g.K2, CK_GATHER_KEY)) key = 0;
       const float4 u = sv.rec[r];
       const uint32_t n0 = sv.K12d.div(key), rem = key - n0 * (uint32_t)(g.K1 * g.K2);
       const uint32_t n1 = sv.K2d.div(rem), n2 = rem - n1 * (uint32_t)g.K2;

@@ -24,6 +24,8 @@
 
 namespace spme {
 
+SPME_CHECK_READER(sort)
+
 constexpr int RS_THREADS = 128;
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_ITEMS = 8;
@@ -260,6 +262,7 @@ size_t cell_count_words(long nb) { return (size_t)(3 * nb + 3 + cell_tiles(nb));
 struct BucketMap {
   FastDiv K2d;
   uint32_t nzb, zshift;
+  uint32_t nb;  // buckets (for the index-checking build)
   __device__ __forceinline__ uint32_t operator()(uint32_t key) const {
     uint32_t row, n2;
     K2d.divmod(key, row, n2);
@@ -272,6 +275,7 @@ static BucketMap bucket_map(const Geom &g, int zshift) {
   m.K2d = FastDiv((uint32_t)g.K2);
   m.nzb = (uint32_t)(((long)g.K2 + (1L << zshift) - 1) >> zshift);
   m.zshift = (uint32_t)zshift;
+  m.nb = (uint32_t)sort_buckets(g, zshift);
   return m;
 }
 
@@ -292,6 +296,7 @@ __global__ void __launch_bounds__(256) key_count_kernel(Geom g, int n, const dou
   uint32_t row, n2;
   bm.K2d.divmod(key, row, n2);
   const uint32_t b = row * bm.nzb + (n2 >> bm.zshift);
+  if (!SPME_IN(b, bm.nb, CK_SORT_BUCKET)) return;
   slot[a] = atomicAdd(&count[b], 1u);
   if (head) {
     const int off = (int)(n2 & ((1u << bm.zshift) - 1u));
@@ -417,8 +422,10 @@ __global__ void __launch_bounds__(256) cell_scatter_kernel(int n, const uint32_t
   if (a >= n) return;
   const uint32_t key = keys[a];
   const uint32_t b = bm(key);
+  if (!SPME_IN(b, bm.nb, CK_SORT_BUCKET)) return;
   const int lo = cs[b], hi = cs[b + 1];
   const int pos = lo + (int)slot[a];
+  if (!SPME_IN(pos - lo, hi - lo, CK_SORT_SCATTER) || !SPME_IN(hi - 1, n, CK_SORT_SCATTER)) return;
   tkeys[pos] = key;
   tmp[pos] = (uint32_t)a;
   if (hi - lo == 1) {
@@ -451,6 +458,7 @@ __device__ void big_cell_sort(int lo, int c, uint32_t *tkeys, uint32_t *tmp, uin
         if (pair_less(sk[m], si[m], vk, vi)) l = m + 1; else h = m;
       }
       const int d = (left ? rs : os) + (i - rs) + (l - os);
+      if (!SPME_IN(d, c, CK_SORT_MERGE)) continue;
       dk[d] = vk;
       di[d] = vi;
     }
@@ -478,16 +486,19 @@ __global__ void __launch_bounds__(256) cell_fixup_kernel(int n, const int *__res
   if (i < n) {
     const uint32_t key = tkeys[i];
     const uint32_t b = bm(key);
-    const int lo = cs[b], c = cs[b + 1] - lo;
+    const bool ok = SPME_IN(b, bm.nb, CK_SORT_BUCKET);
+    const int lo = ok ? cs[b] : 0, c = ok ? cs[b + 1] - lo : 1;
     if (c > kBigCell) {
       if (i == lo) big[atomicAdd(&ctl[0], 1u)] = b;
     } else if (c > 1) {
       const uint32_t a = tmp[i];
       int r = 0;
       for (int j = lo; j < lo + c; j++) r += pair_less(tkeys[j], tmp[j], key, a) ? 1 : 0;
-      skeys[lo + r] = key;
-      perm[lo + r] = a;
-      rec_sorted[lo + r] = rec[a];
+      if (SPME_IN(r, c, CK_SORT_FIXUP) && SPME_IN(lo + c - 1, n, CK_SORT_FIXUP)) {
+        skeys[lo + r] = key;
+        perm[lo + r] = a;
+        rec_sorted[lo + r] = rec[a];
+      }
     }
   }
   // the last CTA to finish sorts the listed large buckets

@@ -34,6 +34,8 @@
 
 namespace spme {
 
+SPME_CHECK_READER(spread)
+
 constexpr int SP_TX = 8, SP_TY = 8, SP_TZ = 32;  // brick of one warp
 constexpr int SP_WARPS = 4;                     // warps per CTA
 
@@ -163,6 +165,7 @@ struct SpArgs {
   float *grid;
   int ntx, nty, ntz, nbricks;
   int nzb;
+  long nb;                // buckets (cs holds nb + 1 offsets; cs[nb] = atoms)
   FastDiv K2d;
 };
 
@@ -210,6 +213,11 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
       const int row = wrap_near(ex, K0, nearx) * K1 + wrap_near(ey, K1, neary);
       const int b0 = row * A.nzb + (n2a >> ZB), b1 = row * A.nzb + ((n2e - 1) >> ZB);
       const uint32_t kbase = (uint32_t)row * (uint32_t)K2;
+      if (!SPME_IN(b0, A.nb, CK_SPREAD_BUCKET) || !SPME_IN(b1, A.nb, CK_SPREAD_BUCKET)) {
+        gr.start[r] = 0;
+        gr.pref[r + 1] = 0;
+        continue;
+      }
       int lo, hi;
       const int lo_off = n2a & (ZW - 1), hi_off = n2e & (ZW - 1);
       if (lo_off == 0) lo = __ldg(A.cs + b0);
@@ -218,6 +226,9 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
       if (hi_off == 0 || n2e == K2) hi = __ldg(A.cs + b1 + 1);
       else if (hi_off == H - 1) hi = __ldg(A.cs + b1) + (int)__ldg(A.head + b1);
       else hi = keys_lower_bound(A.keys, __ldg(A.cs + b1), __ldg(A.cs + b1 + 1), kbase + n2e);
+      if (!SPME_IN(lo - A.cs[b0], A.cs[b1 + 1] - A.cs[b0] + 1, CK_SPREAD_RANGE) ||
+          !SPME_IN(hi - lo, A.cs[b1 + 1] - lo + 1, CK_SPREAD_RANGE))
+        hi = lo;
       gr.start[r] = lo;
       gr.pref[r + 1] = hi - lo;
     }
@@ -243,7 +254,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
     const int w_lo = (int)((long)total * member / NS), w_hi = (int)((long)total * (member + 1) / NS);
     for (int chunk = w_lo; chunk < w_hi; chunk += 32) {
       const int t = chunk + lane;
-      const bool valid = t < w_hi;
+      bool valid = t < w_hi;
       int a = 0, hr = 0, mycase = NC;  // NC: no atom (sorts last, never walked)
       if (valid) {
         int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
@@ -253,9 +264,14 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
         }
         a = gr.start[lo] + (t - gr.pref[lo]);
         hr = lo;
-        uint32_t qk, n2;
-        A.K2d.divmod(__ldg(A.keys + a), qk, n2);
-        mycase = (int)n2 + zoff + P - 1;  // in [0, NC): first z tap rz = mycase - (P - 1)
+        if (SPME_IN(a, A.cs[A.nb], CK_SPREAD_ATOM)) {
+          uint32_t qk, n2;
+          A.K2d.divmod(__ldg(A.keys + a), qk, n2);
+          mycase = (int)n2 + zoff + P - 1;  // in [0, NC): first z tap rz = mycase - (P - 1)
+          if (!SPME_IN(mycase, NC, CK_SPREAD_CASE)) valid = false, mycase = NC;
+        } else {
+          valid = false;
+        }
       }
       // counting sort of the chunk on the window case, ties in lane order:
       // cnt[c] = atoms of case c, then (exclusive scan) the first row of case c
@@ -279,7 +295,8 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
       }
       __syncwarp();
       if (valid) {
-        const int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
+        int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
+        if (!SPME_IN(row, 32, CK_SPREAD_ROW)) row = 0;
         const float4 u = __ldg(A.rec + a);
         // tap i of each axis: the weight of point first + i, M(f + P - 1 - i)
 #pragma unroll
@@ -290,7 +307,8 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
           st.zp[row][i] = pack2(wz, wz);
         }
         // the brick's column c takes tap c - (rx - P + 1): scratch [OFF + P - 1 - rx + c]
-        const int bx = OFF + P - 1 - hr / RY, by = OFF + P - 1 - hr % RY;
+        int bx = OFF + P - 1 - hr / RY, by = OFF + P - 1 - hr % RY;
+        if (!SPME_IN(bx, C::SL - 7, CK_SPREAD_TAP) || !SPME_IN(by, C::SL - 7, CK_SPREAD_TAP)) bx = by = 0;
 #pragma unroll
         for (int c = 0; c < 4; c++) st.wxl[row][c] = pack2(st.sx[lane][bx + 2 * c], st.sx[lane][bx + 2 * c + 1]);
 #pragma unroll
@@ -310,6 +328,7 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
       const int gx = x0 + 2 * lx + c, gy = y0 + ly;
       if (gx >= K0 || gy >= K1) continue;
       float *col = A.grid + ((long)gx * K1 + gy) * K2 + z0;
+      if (!SPME_IN(((long)gx * K1 + gy) * K2 + min(z0 + SP_TZ, K2) - 1, (long)K0 * K1 * K2, CK_SPREAD_GRID)) continue;
       if ((K2 & 3) == 0 && z0 + SP_TZ <= K2) {
 #pragma unroll
         for (int z = 0; z < SP_TZ; z += 4) {
@@ -418,6 +437,7 @@ int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const u
   A.ntz = (g.K2 + SP_TZ - 1) / SP_TZ;
   A.nbricks = A.ntx * A.nty * A.ntz;
   A.nzb = (g.K2 + (1 << kSpreadZShift) - 1) >> kSpreadZShift;
+  A.nb = nb;
   A.K2d = FastDiv((uint32_t)g.K2);
   // Split a brick's atoms over more warps while the bricks alone would not
   // fill the SMs (5 CTAs of 4 warps resident per SM).

@@ -28,6 +28,10 @@
 #include "../../include/sfac.h"
 #include "spme_kernels.hpp"
 
+namespace spme {
+SPME_CHECK_READER(serve)
+}  // namespace spme
+
 namespace {
 
 constexpr int kHdr = 16;  // header doubles of a packed request: L[6], n, fractional flag, unused
@@ -41,6 +45,7 @@ constexpr int kHdr = 16;  // header doubles of a packed request: L[6], n, fracti
 __global__ void unpack_kernel(const double *__restrict__ blk, double *__restrict__ x, double *__restrict__ q,
                               int ncap) {
   const int n = (int)blk[6];
+  if (n > 0 && !SPME_IN(n - 1, ncap, spme::CK_SERVE_ATOM)) return;
   const bool frac = blk[7] != 0.0;
   const double L0 = blk[0], L1 = blk[1], L2 = blk[2], L3 = blk[3], L4 = blk[4], L5 = blk[5];
   const double *xs = blk + kHdr, *qs = xs + 3 * (size_t)n;
@@ -65,8 +70,9 @@ __global__ void unpack_kernel(const double *__restrict__ blk, double *__restrict
 // phi of the first n atoms behind their dE/dx in the output block
 // [E, vir(6), dx(3n), phi(n)] (dx already sits at out + 7).
 __global__ void pack_phi_kernel(const double *__restrict__ blk, const double *__restrict__ phi,
-                                double *__restrict__ out) {
+                                double *__restrict__ out, int ncap) {
   const int n = (int)blk[6];
+  if (n > 0 && !SPME_IN(n - 1, ncap, spme::CK_SERVE_OUT)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[7 + 3 * (size_t)n + i] = phi[i];
 }
@@ -172,7 +178,7 @@ bool enqueue_request_work(Slot *s) {
   unpack_kernel<<<blocks, 256, 0, s->st>>>(s->d_blk, s->d_x, s->d_q, s->ncap);
   if (sfac_box_update_device(s->h, s->d_blk) != 0) return false;
   if (sfac_solve_device(s->h, s->ncap, s->d_x, s->d_q, s->d_out + 7, s->d_phi, s->d_out) != 0) return false;
-  pack_phi_kernel<<<blocks, 256, 0, s->st>>>(s->d_blk, s->d_phi, s->d_out);
+  pack_phi_kernel<<<blocks, 256, 0, s->st>>>(s->d_blk, s->d_phi, s->d_out, s->ncap);
   return cudaGetLastError() == cudaSuccess;
 }
 

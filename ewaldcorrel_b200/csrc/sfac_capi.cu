@@ -44,6 +44,15 @@ cudaError_t device_malloc(void **p, size_t bytes) {
   return cudaMalloc(p, bytes);
 }
 
+SPME_CHECK_READER(capi)
+
+// Exercises the check machinery: a logical bound of 32 on a 64-float buffer,
+// index 40 -- the check fails and skips the store, which would have stayed
+// inside the allocation anyway.
+__global__ void check_selftest_kernel(float *buf) {
+  if (threadIdx.x == 0 && SPME_IN(40, 32, CK_SELFTEST)) buf[40] = 1.f;
+}
+
 }  // namespace spme
 
 namespace {
@@ -1196,6 +1205,43 @@ int sfac_debug_sort(void *p, int n, int *keys, int *perm) {
       !CK(h, cudaMemcpyAsync(perm, h->sb.vals[h->sb.cur], sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream)))
     return 1;
   return sync(h) ? 0 : 1;
+}
+
+int sfac_check_enabled(void) {
+#ifdef SPME_CHECK
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+int sfac_check_take(unsigned long long *word) {
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  unsigned long long (*const take[])() = {spme::check_take_sort,  spme::check_take_spread,
+                                          spme::check_take_gather, spme::check_take_fft,
+                                          spme::check_take_serve,  spme::check_take_capi};
+  int first = 0;
+  for (int m = 0; m < (int)(sizeof(take) / sizeof(take[0])); m++) {
+    const unsigned long long v = take[m]();
+    if (v && !first) {
+      first = m + 1;
+      if (word) *word = v;
+    }
+  }
+  return first;
+}
+
+int sfac_check_selftest(void) {
+  if (!sfac_check_enabled()) return -1;
+  float *buf = nullptr;
+  if (cudaMalloc(&buf, 64 * sizeof(float)) != cudaSuccess) return 2;
+  unsigned long long w = 0;
+  sfac_check_take(nullptr);  // start from clear words
+  spme::check_selftest_kernel<<<1, 32>>>(buf);
+  const int m = sfac_check_take(&w);
+  cudaFree(buf);
+  const unsigned long long want = ((unsigned long long)spme::CK_SELFTEST << 40) | 40ull;
+  return (m == 6 && w == want) ? 0 : 1;
 }
 
 int sfac_debug_fail_alloc(int nth) {

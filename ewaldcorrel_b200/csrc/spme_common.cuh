@@ -37,6 +37,45 @@ struct Spline {
 
 __host__ __device__ inline int imod(int a, int b) { return ((a % b) + b) % b; }
 
+// Index-checking build (-DSPME_CHECK).  SPME_IN(i, n, site) is true when
+// 0 <= i < n.  Otherwise the module's error word records the first failure
+// (site << 40 | the index's low 40 bits) and the caller skips the access:
+// no trap, the context stays usable, and the host reads the word with
+// sfac_check_take.  The product build compiles every check to `true`.
+enum CheckSite : unsigned {
+  CK_SORT_BUCKET = 0x101, CK_SORT_SCATTER, CK_SORT_FIXUP, CK_SORT_MERGE,
+  CK_SPREAD_BUCKET = 0x201, CK_SPREAD_RANGE, CK_SPREAD_ATOM, CK_SPREAD_CASE, CK_SPREAD_ROW,
+  CK_SPREAD_TAP, CK_SPREAD_GRID,
+  CK_GATHER_ATOM = 0x301, CK_GATHER_KEY, CK_GATHER_GRID,
+  CK_FFT_LINE = 0x401, CK_FFT_CONV,
+  CK_SERVE_ATOM = 0x501, CK_SERVE_OUT,
+  CK_SELFTEST = 0xf01,
+};
+#ifdef SPME_CHECK
+static __device__ unsigned long long spme_check_word;
+__device__ __noinline__ static bool spme_check_fail(long long i, unsigned site) {
+  const unsigned long long w = ((unsigned long long)site << 40) | ((unsigned long long)i & ((1ull << 40) - 1));
+  atomicCAS(&spme_check_word, 0ull, w);
+  return false;
+}
+#define SPME_IN(i, n, site)                                                                       \
+  ((unsigned long long)(long long)(i) < (unsigned long long)(long long)(n) ? true                  \
+                                                                            : spme::spme_check_fail( \
+                                                                                  (long long)(i), (site)))
+// Host: reads and clears this module's word (after the device is idle).
+#define SPME_CHECK_READER(name)                                          \
+  unsigned long long check_take_##name() {                               \
+    unsigned long long v = 0, z = 0;                                     \
+    if (cudaMemcpyFromSymbol(&v, spme_check_word, sizeof v) != cudaSuccess) return 0; \
+    if (v) cudaMemcpyToSymbol(spme_check_word, &z, sizeof z);           \
+    return v;                                                            \
+  }
+#else
+#define SPME_IN(i, n, site) true
+#define SPME_CHECK_READER(name) \
+  unsigned long long check_take_##name() { return 0; }
+#endif
+
 // Division by a runtime-invariant positive integer d with a multiply-high and
 // a shift (the round-up multiplier method of Granlund and Montgomery): for
 // 0 <= x < 2^31, q = umulhi(x, m) >> s equals x / d exactly.

@@ -14,6 +14,15 @@ namespace spme {
 // (sfac_debug_fail_alloc) and check the error paths without a GPU fault.
 cudaError_t device_malloc(void **p, size_t bytes);
 
+// Index-checking build: each kernel module's error word, read and cleared
+// (0 when no check failed, and always 0 in the product build).
+unsigned long long check_take_sort();
+unsigned long long check_take_spread();
+unsigned long long check_take_gather();
+unsigned long long check_take_fft();
+unsigned long long check_take_serve();
+unsigned long long check_take_capi();
+
 // ---- sort (k_sort.cu) ----
 struct SortBuffers {
   uint32_t *keys[2];   // [1]: cell key of every atom (input order); [0]: keys in cell order

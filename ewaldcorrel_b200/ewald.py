@@ -26,11 +26,13 @@ _LIB = None
 
 
 def _load():
-    """Loads libsfac.so from this directory; fails loudly if it is not built."""
+    """Loads libsfac.so from this directory (or the library file that
+    EWALDCORREL_LIBSFAC names, e.g. the index-checking libsfac_check.so);
+    fails loudly if it is not built."""
     global _LIB
     if _LIB is None:
         here = os.path.dirname(os.path.abspath(__file__))
-        path = os.path.join(here, "libsfac.so")
+        path = os.environ.get("EWALDCORREL_LIBSFAC") or os.path.join(here, "libsfac.so")
         if not os.path.exists(path):
             raise RuntimeError(
                 f"{path} is not built: run `python -m ewaldcorrel_b200.build` (needs nvcc)")

@@ -311,6 +311,22 @@ int sfac_debug_sort(void *sfac, int n, int *keys, int *perm);
  * returning NULL, set_A returning 2, spme_server_submit returning 2) without
  * exhausting a GPU.  Returns 0. */
 int sfac_debug_fail_alloc(int nth);
+/* Index-checking build (libsfac_check.so, compiled with -DSPME_CHECK): the
+ * kernels test their grid, bucket, atom and table indices; a failed check
+ * records (site << 40 | index) in its module's error word and skips the
+ * access instead of trapping.
+ * sfac_check_enabled: 1 in the checking build, 0 in the product build.
+ * sfac_check_take: after a device synchronize, reads and clears every
+ *   module's word; returns 0 if no check failed since the last call, else
+ *   the first failing module (1 sort, 2 spread, 3 gather, 4 FFT and
+ *   convolution, 5 serving, 6 C API) with its word in *word (may be NULL);
+ *   -1 if the device reports an error.
+ * sfac_check_selftest: runs one check that must fail (its store stays inside
+ *   its buffer either way) and returns 0 if the word came back as expected,
+ *   1 if not, 2 on allocation failure, -1 in the product build. */
+int sfac_check_enabled(void);
+int sfac_check_take(unsigned long long *word);
+int sfac_check_selftest(void);
 int sfac_debug_spread(void *sfac, float *grid);
 
 #ifdef __cplusplus

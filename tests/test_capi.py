@@ -84,6 +84,22 @@ def _has_gpu():
 
 
 @pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU error path")
+def test_only_the_checking_build_checks(libsfac_path):
+    """sfac_check_enabled makes no CUDA call: 0 in the product library, 1 in
+    the index-checking one (-DSPME_CHECK), which exports the same symbols."""
+    import ctypes
+
+    from ewaldcorrel_b200 import build
+
+    assert ctypes.CDLL(libsfac_path).sfac_check_enabled() == 0
+    if not os.path.exists(build.LIB_CHECK):
+        pytest.skip("libsfac_check.so not built")
+    chk = ctypes.CDLL(build.LIB_CHECK)
+    assert chk.sfac_check_enabled() == 1
+    for name in declared_functions():
+        assert hasattr(chk, name), name
+
+
 def test_ctor_without_gpu_returns_null(libsfac_path):
     from ewaldcorrel_b200 import ewald
 
