@@ -6,27 +6,30 @@
 // order^3 neighbouring cells in a fixed order.  No atomics, so the grid is
 // bit-for-bit reproducible.
 //
-// Blocking: a warp owns an 8 x 8 x 32 brick of grid points in registers.
+// Blocking: a warp owns an 8 x 8 x 16 brick of grid points in registers.
 // Lane (lx, ly) holds the two neighbouring columns x = 2 lx, 2 lx + 1 at
-// y = ly, 32 z points each, as 32 packed FP32 pairs, so that one packed FMA
-// (fma.rn.f32x2) adds an atom's z tap to both columns.  The atoms of the
-// brick's halo (the cells whose stencils reach it) are the sorted atoms of
-// (x, y) cell rows, found through the bucket offsets of the cell sort (runs
-// of 32 z cells per row); an interior brick's halo starts H = p/2 cells
-// before a bucket boundary and ends H - 1 cells after one, and the sort's
-// per-bucket head/tail counts give those cuts without a search.
+// y = ly, 16 z points each, as 16 packed FP32 pairs, so that one packed FMA
+// (fma.rn.f32x2) adds an atom's z tap to both columns.  The brick is 16
+// deep rather than 32 so that the kernel fits in 64 registers: 8 CTAs of 4
+// warps per SM hide the shared-memory latency of the walk better than 5 at
+// 96 registers outweigh the longer z halo.  The atoms of the brick's halo
+// (the cells whose stencils reach it) are the sorted atoms of (x, y) cell
+// rows, found through the bucket offsets of the cell sort (runs of 32 z
+// cells per row); a brick's halo starts H = p/2 cells before a bucket
+// boundary (even bricks) or ends H - 1 cells after one (odd bricks), where
+// the sort's per-bucket tail/head counts give the cut without a search.
 //
 // The atoms are staged 32 at a time, one per lane, at the row given by a
 // counting sort of the chunk on its window case (the place of the atom's z
 // taps in the brick, the same for every lane; ties in lane order).  Staging
 // evaluates the order-p B-spline taps of the three fractions (the charge
-// folded into x) once and stores what the lanes will read: the weight of
-// each of the brick's 8 x columns (as the 4 pairs the lanes hold) and 8 y
-// rows -- zero where the atom's stencil misses -- and the z taps as
-// duplicated pairs ready for the packed FMA.  The walk goes window case by
-// window case in a compile-time unrolled chain, each case a plain loop over
-// its contiguous rows: per atom, the lane's x pair and y weight, two
-// multiplies, the z taps and p packed FMAs into fixed registers -- no
+// folded into x) once and stores what the lanes will read: the weights of
+// the brick's 8 x columns (as the 4 pairs the lanes hold) and 8 y rows,
+// written straight to their columns of the row after zeroing it, and the z
+// taps as duplicated pairs ready for the packed FMA.  The walk goes window
+// case by window case in a compile-time unrolled chain, each case a plain
+// loop over its contiguous rows: per atom, the lane's x pair and y weight,
+// two multiplies, the z taps and p packed FMAs into fixed registers -- no
 // indirect jump, no divergent branch.  Small grids split one brick's atoms
 // over 2 or 4 warps (equal contiguous shares, summed in warp order through
 // shared memory: still a fixed order).
@@ -36,7 +39,8 @@ namespace spme {
 
 SPME_CHECK_READER(spread)
 
-constexpr int SP_TX = 8, SP_TY = 8, SP_TZ = 32;  // brick of one warp
+constexpr int SP_TX = 8, SP_TY = 8, SP_TZ = 16;  // brick of one warp
+constexpr int SP_MIN_CTAS = 8;                  // resident CTAs per SM (64 registers)
 constexpr int SP_WARPS = 4;                     // warps per CTA
 
 typedef unsigned long long f2r;  // two FP32 values in one 64-bit register (low word first)
@@ -62,10 +66,6 @@ struct SpCfg {
   // halo cell rows of a brick: cells [x0 - H, x0 + TX - 2 + H] (RX of them)
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
   static constexpr int NC = SP_TZ + P - 1;  // window cases: first z tap rz in [1 - P, TZ - 1]
-  // Scratch tap rows: tap i at [OFF + i], zero elsewhere; column c of the
-  // brick (0..7) reads [OFF + P - 1 - r + c] for the atom's halo row r.
-  static constexpr int OFF = 7;
-  static constexpr int SL = (P + 14) | 1;
   static constexpr int ZL = (P + 1) / 2 * 2;  // z pairs per atom (even: rows stay 16-byte aligned)
 };
 
@@ -74,24 +74,23 @@ template <int P>
 struct SpStage {
   using C = SpCfg<P>;
   f2r zp[32][C::ZL];   // (wz[t], wz[t]), t < P: weight of z = rz + t
-  f2r wxl[32][5];      // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 5 pairs)
-  float wyl[32][9];    // y weights of rows 0..7 (padded to 9)
+  __align__(16) f2r wxl[32][6];   // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 6 pairs)
+  __align__(16) float wyl[32][12]; // y weights of rows 0..7 (padded to 12)
   int cnt[64];         // atoms per window case in the chunk, then the case starts
-  float sx[32][C::SL]; // per-lane scratch: zero-padded x taps (charge included)
-  float sy[32][C::SL]; // per-lane scratch: zero-padded y taps
 };
 template <int P>
 struct SpGroup {  // per brick: the halo rows' atom ranges of one z piece
   int start[SpCfg<P>::NR];
   int pref[SpCfg<P>::NR + 1];
 };
-template <int P>
+template <int P, int NS>
 constexpr size_t sp_stage_bytes() {
-  return sizeof(SpStage<P>) > 64 * 33 * 4 ? sizeof(SpStage<P>) : 64 * 33 * 4;
+  if (NS == 1) return sizeof(SpStage<P>);
+  return sizeof(SpStage<P>) > 2 * SP_TZ * 33 * 4 ? sizeof(SpStage<P>) : 2 * SP_TZ * 33 * 4;
 }
-template <int P>
+template <int P, int NS>
 constexpr size_t sp_smem_bytes() {
-  return SP_WARPS * (sp_stage_bytes<P>() + sizeof(SpGroup<P>));
+  return SP_WARPS * (sp_stage_bytes<P, NS>() + sizeof(SpGroup<P>));
 }
 
 // acc[z] += wxy * zp[t] for the taps t whose z = C - (P - 1) + t lies in the
@@ -170,15 +169,15 @@ struct SpArgs {
 };
 
 template <int P, int NS>
-__global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spline S) {
+__global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpArgs A, Spline S) {
   using C = SpCfg<P>;
-  constexpr int H = C::H, RX = C::RX, RY = C::RY, NR = C::NR, OFF = C::OFF, NC = C::NC;
-  constexpr int ZB = 5, ZW = 1 << ZB;  // bucket: 32 z cells
+  constexpr int H = C::H, RX = C::RX, RY = C::RY, NR = C::NR, NC = C::NC;
+  constexpr int ZB = kSpreadZShift, ZW = 1 << ZB;  // bucket of the sort: 32 z cells
   extern __shared__ __align__(16) unsigned char sp_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int group = warp / NS, member = warp % NS;
-  SpStage<P> &st = *reinterpret_cast<SpStage<P> *>(sp_smem + warp * sp_stage_bytes<P>());
-  SpGroup<P> &gr = *reinterpret_cast<SpGroup<P> *>(sp_smem + SP_WARPS * sp_stage_bytes<P>() +
+  SpStage<P> &st = *reinterpret_cast<SpStage<P> *>(sp_smem + warp * sp_stage_bytes<P, NS>());
+  SpGroup<P> &gr = *reinterpret_cast<SpGroup<P> *>(sp_smem + SP_WARPS * sp_stage_bytes<P, NS>() +
                                                    group * sizeof(SpGroup<P>));
   const long brick = (long)blockIdx.x * (SP_WARPS / NS) + group;
   if (brick >= A.nbricks) return;  // the whole group leaves together
@@ -190,11 +189,6 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
   const int gt = member * 32 + lane, gn = 32 * NS;  // thread index and size of the group
   const bool nearx = K0 >= RX, neary = K1 >= RY;
 
-  // zero this lane's scratch rows once (staging writes only the tap positions)
-  for (int i = 0; i < C::SL; i++) {
-    st.sx[lane][i] = 0.f;
-    st.sy[lane][i] = 0.f;
-  }
 
   f2r acc[SP_TZ];
 #pragma unroll
@@ -298,21 +292,25 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
         int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
         if (!SPME_IN(row, 32, CK_SPREAD_ROW)) row = 0;
         const float4 u = __ldg(A.rec + a);
-        // tap i of each axis: the weight of point first + i, M(f + P - 1 - i)
+        // tap i of each axis: the weight of point first + i, M(f + P - 1 - i);
+        // the brick's column c = i + rx - (P - 1) takes tap i (zero elsewhere)
+        float *wxr = reinterpret_cast<float *>(&st.wxl[row][0]);
+        float *wyr = &st.wyl[row][0];
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4 *>(wxr)[0] = z4;
+        reinterpret_cast<float4 *>(wxr)[1] = z4;
+        reinterpret_cast<float4 *>(wyr)[0] = z4;
+        reinterpret_cast<float4 *>(wyr)[1] = z4;
+        const int cx = hr / RY - (P - 1), cy = hr % RY - (P - 1);
 #pragma unroll
         for (int i = 0; i < P; i++) {
-          st.sx[lane][OFF + i] = u.w * bspl_eval(S, P, u.x, P - 1 - i);
-          st.sy[lane][OFF + i] = bspl_eval(S, P, u.y, P - 1 - i);
+          const float wx = u.w * bspl_eval(S, P, u.x, P - 1 - i);
+          const float wy = bspl_eval(S, P, u.y, P - 1 - i);
           const float wz = bspl_eval(S, P, u.z, P - 1 - i);
+          if ((unsigned)(cx + i) < 8u) wxr[cx + i] = wx;
+          if ((unsigned)(cy + i) < 8u) wyr[cy + i] = wy;
           st.zp[row][i] = pack2(wz, wz);
         }
-        // the brick's column c takes tap c - (rx - P + 1): scratch [OFF + P - 1 - rx + c]
-        int bx = OFF + P - 1 - hr / RY, by = OFF + P - 1 - hr % RY;
-        if (!SPME_IN(bx, C::SL - 7, CK_SPREAD_TAP) || !SPME_IN(by, C::SL - 7, CK_SPREAD_TAP)) bx = by = 0;
-#pragma unroll
-        for (int c = 0; c < 4; c++) st.wxl[row][c] = pack2(st.sx[lane][bx + 2 * c], st.sx[lane][bx + 2 * c + 1]);
-#pragma unroll
-        for (int c = 0; c < 8; c++) st.wyl[row][c] = st.sy[lane][by + c];
       }
       __syncwarp();
       sp_walk<P, 0>(acc, st, lx, ly, 0);
@@ -355,21 +353,21 @@ __global__ void __launch_bounds__(SP_WARPS * 32, 5) spread_kernel(SpArgs A, Spli
     // group's warps in warp order, stored with consecutive threads on
     // consecutive z (coalesced)
     group_sync<NS>(group);
-    float *part = reinterpret_cast<float *>(&st);  // [k * 32 + z][33]: column 2 lx + k of lane
+    float *part = reinterpret_cast<float *>(&st);  // [k * SP_TZ + z][33]: column 2 lx + k of lane
 #pragma unroll
     for (int z = 0; z < SP_TZ; z++) {
       float v0, v1;
       unpack2(acc[z], v0, v1);
       part[z * 33 + lane] = v0;
-      part[(32 + z) * 33 + lane] = v1;
+      part[(SP_TZ + z) * 33 + lane] = v1;
     }
     group_sync<NS>(group);
-    const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * NS * sp_stage_bytes<P>());
-    const size_t mstride = sp_stage_bytes<P>() / sizeof(float);
+    const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * NS * sp_stage_bytes<P, NS>());
+    const size_t mstride = sp_stage_bytes<P, NS>() / sizeof(float);
     for (int p = gt; p < SP_TX * SP_TY * SP_TZ; p += gn) {
-      const int z = p & 31, col = p >> 5;
+      const int z = p % SP_TZ, col = p / SP_TZ;
       const int xr = col >> 3, yr = col & 7;
-      const int src = ((xr & 1) * 32 + z) * 33 + (xr >> 1) + 4 * yr;
+      const int src = ((xr & 1) * SP_TZ + z) * 33 + (xr >> 1) + 4 * yr;
       float v = gpart[src];
 #pragma unroll
       for (int m = 1; m < NS; m++) v += gpart[m * mstride + src];
@@ -383,7 +381,7 @@ template <int P, int NS>
 static void spread_ps(const SpArgs &A, const Spline &S, cudaStream_t st) {
   constexpr int per_cta = SP_WARPS / NS;
   const long ctas = (A.nbricks + per_cta - 1) / per_cta;
-  spread_kernel<P, NS><<<(unsigned)ctas, SP_WARPS * 32, sp_smem_bytes<P>(), st>>>(A, S);
+  spread_kernel<P, NS><<<(unsigned)ctas, SP_WARPS * 32, sp_smem_bytes<P, NS>(), st>>>(A, S);
 }
 
 template <int P>
@@ -395,9 +393,9 @@ static void spread_p(const SpArgs &A, int nsplit, const Spline &S, cudaStream_t 
 
 template <int P>
 static void spread_attr() {
-  cudaFuncSetAttribute(spread_kernel<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
-  cudaFuncSetAttribute(spread_kernel<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
-  cudaFuncSetAttribute(spread_kernel<P, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P>());
+  cudaFuncSetAttribute(spread_kernel<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P, 1>());
+  cudaFuncSetAttribute(spread_kernel<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P, 2>());
+  cudaFuncSetAttribute(spread_kernel<P, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp_smem_bytes<P, 4>());
 }
 
 void spread_prepare() {
@@ -422,7 +420,7 @@ static int sm_count() {
 
 int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const uint32_t *keys_sorted,
                   const float4 *rec_sorted, float *grid, cudaStream_t st) {
-  static_assert(kSpreadZShift == 5, "the spread's bricks are 32 cells deep, one bucket");
+  static_assert((1 << kSpreadZShift) % SP_TZ == 0, "a brick's z range lies within one bucket");
   SpArgs A{};
   A.g = g;
   A.cs = cell_start;
@@ -441,7 +439,7 @@ int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const u
   A.K2d = FastDiv((uint32_t)g.K2);
   // Split a brick's atoms over more warps while the bricks alone would not
   // fill the SMs (5 CTAs of 4 warps resident per SM).
-  const long want = (long)sm_count() * 20;
+  const long want = (long)sm_count() * SP_WARPS * SP_MIN_CTAS;
   int nsplit = 1;
   while (nsplit < SP_WARPS && (long)A.nbricks * nsplit < want) nsplit *= 2;
   switch (g.order) {

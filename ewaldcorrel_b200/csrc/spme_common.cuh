@@ -45,7 +45,7 @@ __host__ __device__ inline int imod(int a, int b) { return ((a % b) + b) % b; }
 enum CheckSite : unsigned {
   CK_SORT_BUCKET = 0x101, CK_SORT_SCATTER, CK_SORT_FIXUP, CK_SORT_MERGE,
   CK_SPREAD_BUCKET = 0x201, CK_SPREAD_RANGE, CK_SPREAD_ATOM, CK_SPREAD_CASE, CK_SPREAD_ROW,
-  CK_SPREAD_TAP, CK_SPREAD_GRID,
+  CK_SPREAD_GRID,
   CK_GATHER_ATOM = 0x301, CK_GATHER_KEY, CK_GATHER_GRID,
   CK_FFT_LINE = 0x401, CK_FFT_CONV,
   CK_SERVE_ATOM = 0x501, CK_SERVE_OUT,
