@@ -287,6 +287,17 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
         st.cnt[2 * lane] = incl - e0 - e1;
         st.cnt[2 * lane + 1] = incl - e1;
       }
+      // zero the chunk's x/y weight rows with contiguous stores of the whole warp
+      {
+        float4 *zx = reinterpret_cast<float4 *>(&st.wxl[0][0]);
+        float4 *zy = reinterpret_cast<float4 *>(&st.wyl[0][0]);
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int v = 0; v < 3; v++) {
+          zx[v * 32 + lane] = z4;
+          zy[v * 32 + lane] = z4;
+        }
+      }
       __syncwarp();
       if (valid) {
         int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
@@ -296,12 +307,9 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
         // the brick's column c = i + rx - (P - 1) takes tap i (zero elsewhere)
         float *wxr = reinterpret_cast<float *>(&st.wxl[row][0]);
         float *wyr = &st.wyl[row][0];
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        reinterpret_cast<float4 *>(wxr)[0] = z4;
-        reinterpret_cast<float4 *>(wxr)[1] = z4;
-        reinterpret_cast<float4 *>(wyr)[0] = z4;
-        reinterpret_cast<float4 *>(wyr)[1] = z4;
         const int cx = hr / RY - (P - 1), cy = hr % RY - (P - 1);
+        static_assert(SpCfg<P>::ZL == P, "even orders: the z taps fill whole 16-byte pairs");
+        float zt[P];
 #pragma unroll
         for (int i = 0; i < P; i++) {
           const float wx = u.w * bspl_eval(S, P, u.x, P - 1 - i);
@@ -309,8 +317,12 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
           const float wz = bspl_eval(S, P, u.z, P - 1 - i);
           if ((unsigned)(cx + i) < 8u) wxr[cx + i] = wx;
           if ((unsigned)(cy + i) < 8u) wyr[cy + i] = wy;
-          st.zp[row][i] = pack2(wz, wz);
+          zt[i] = wz;
         }
+#pragma unroll
+        for (int v = 0; v < SpCfg<P>::ZL / 2; v++)
+          *reinterpret_cast<ulonglong2 *>(&st.zp[row][2 * v]) =
+              make_ulonglong2(pack2(zt[2 * v], zt[2 * v]), pack2(zt[2 * v + 1], zt[2 * v + 1]));
       }
       __syncwarp();
       sp_walk<P, 0>(acc, st, lx, ly, 0);
