@@ -78,10 +78,13 @@ struct SpStage {
   __align__(16) float wyl[32][12]; // y weights of rows 0..7 (padded to 12)
   int cnt[64];         // atoms per window case in the chunk, then the case starts
 };
+constexpr int kRowMap = 512;
+static_assert(SpCfg<8>::NR <= 256, "halo rows fit a byte");
 template <int P>
 struct SpGroup {  // per brick: the halo rows' atom ranges of one z piece
   int start[SpCfg<P>::NR];
   int pref[SpCfg<P>::NR + 1];
+  uint8_t rowmap[kRowMap];  // halo row of each of the piece's atoms (pieces of at most kRowMap atoms)
 };
 template <int P, int NS>
 constexpr size_t sp_stage_bytes() {
@@ -245,22 +248,37 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
     group_sync<NS>(group);
     const int total = gr.pref[NR];
     const int zoff = ezs - n2a + 1 - H - z0;  // first z tap of an atom in stored cell n2: n2 + zoff
+    const bool mapped = total <= kRowMap;
+    if (mapped) {
+      for (int r = gt; r < NR; r += gn)
+        for (int k = gr.pref[r], e = gr.pref[r + 1]; k < e; k++) gr.rowmap[k] = (uint8_t)r;
+      group_sync<NS>(group);
+    }
     const int w_lo = (int)((long)total * member / NS), w_hi = (int)((long)total * (member + 1) / NS);
     for (int chunk = w_lo; chunk < w_hi; chunk += 32) {
       const int t = chunk + lane;
       bool valid = t < w_hi;
       int a = 0, hr = 0, mycase = NC;  // NC: no atom (sorts last, never walked)
+      float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
       if (valid) {
-        int lo = 0, hi = NR - 1;  // largest r with pref[r] <= t
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (gr.pref[mid] <= t) lo = mid; else hi = mid - 1;
+        int lo;
+        if (mapped) {
+          lo = gr.rowmap[t];
+        } else {
+          lo = 0;  // largest r with pref[r] <= t
+          int hi = NR - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (gr.pref[mid] <= t) lo = mid; else hi = mid - 1;
+          }
         }
         a = gr.start[lo] + (t - gr.pref[lo]);
         hr = lo;
         if (SPME_IN(a, A.cs[A.nb], CK_SPREAD_ATOM)) {
           uint32_t qk, n2;
-          A.K2d.divmod(__ldg(A.keys + a), qk, n2);
+          const uint32_t key = __ldg(A.keys + a);
+          u = __ldg(A.rec + a);
+          A.K2d.divmod(key, qk, n2);
           mycase = (int)n2 + zoff + P - 1;  // in [0, NC): first z tap rz = mycase - (P - 1)
           if (!SPME_IN(mycase, NC, CK_SPREAD_CASE)) valid = false, mycase = NC;
         } else {
@@ -302,7 +320,6 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
       if (valid) {
         int row = st.cnt[mycase] + __popc(peers & ((1u << lane) - 1u));
         if (!SPME_IN(row, 32, CK_SPREAD_ROW)) row = 0;
-        const float4 u = __ldg(A.rec + a);
         // tap i of each axis: the weight of point first + i, M(f + P - 1 - i);
         // the brick's column c = i + rx - (P - 1) takes tap i (zero elsewhere)
         float *wxr = reinterpret_cast<float *>(&st.wxl[row][0]);
@@ -450,7 +467,7 @@ int launch_spread(const Geom &g, const Spline &S, const int *cell_start, const u
   A.nb = nb;
   A.K2d = FastDiv((uint32_t)g.K2);
   // Split a brick's atoms over more warps while the bricks alone would not
-  // fill the SMs (5 CTAs of 4 warps resident per SM).
+  // fill the SMs (SP_MIN_CTAS CTAs of 4 warps resident per SM).
   const long want = (long)sm_count() * SP_WARPS * SP_MIN_CTAS;
   int nsplit = 1;
   while (nsplit < SP_WARPS && (long)A.nbricks * nsplit < want) nsplit *= 2;
