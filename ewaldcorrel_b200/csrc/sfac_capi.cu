@@ -963,7 +963,10 @@ int sfac_set_ewald(void *p, double beta, double max_m) {
   if (h->ewald_src == 2) table = compact = false;  // the box may change on the device (sfac_box_update_device)
   if (const char *e = getenv("SFAC_EWALD_TABLE")) {
     if (e[0] == '0' && e[1] == 0) table = compact = false;  // evaluate the images in every solve
-    if (e[0] == 'c' && e[1] == 0) table = !(compact = true);  // compact table whatever the size
+    if (e[0] == 'c' && e[1] == 0) {  // compact table whatever the size
+      compact = true;
+      table = false;
+    }
   }
   if (table) {
     if (!h->d_A && !dalloc(h, &h->d_A, 7 * nm)) return 2;
