@@ -179,15 +179,16 @@ def algorithmic_bytes(n, K):
 # DRAM bytes (read + write) per launch of each stage's kernels, from ncu
 # captures of a plain solve (cold caches; summaries in profiles/).  Writes
 # that stay in the 126 MB L2 past the kernel's end are not counted.  At 256^3
-# the spread's figure is from profiles/ncu_full_spread_triclinic1m.md, the x
-# pass's and the gather's from profiles/ncu_full_gather_x2_triclinic1m.md, the
-# z/y passes' from profiles/dram_per_kernel_water_triclinic_fft_gather.md; the
-# water box's from profiles/dram_per_kernel_water.md.  None: not captured for
-# the current kernels.
+# the sort's figure is from profiles/dram_sort_triclinic1m.md, the spread's
+# from profiles/ncu_full_spread_triclinic1m.md, the x pass's and the gather's
+# from profiles/ncu_full_gather_x2_triclinic1m.md, the z/y passes' from
+# profiles/dram_per_kernel_water_triclinic_fft_gather.md; the water box's from
+# profiles/dram_per_kernel_water.md.  None: not captured for the current
+# kernels.
 NCU_TRAFFIC = {
     "water": {"cell_sort": 7.48e6, "spread": None, "fft_forward": 7.30e6, "convolution": 29.00e6,
               "fft_inverse": 7.38e6, "gather": None},
-    "triclinic": {"cell_sort": None, "spread": 46.51e6, "fft_forward": 163.58e6, "convolution": 162.71e6,
+    "triclinic": {"cell_sort": 119.30e6, "spread": 46.51e6, "fft_forward": 163.58e6, "convolution": 162.71e6,
                   "fft_inverse": 165.67e6, "gather": 160.72e6},
 }
 # Kernels of each stage (the roofline is reported for the longest stage that
