@@ -541,9 +541,12 @@ int launch_cell_sort(const Geom &g, int n, const double *x, const double *w, Sor
                                                        ht_h ? head : nullptr, tail, ht_h);
     launches++;
   }
-  tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);
+  if (ntiles > 1) {  // one tile (grids up to about 64^3): its scan starts from 0, no tile sums needed
+    tile_sum_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);
+    launches++;
+  }
   cell_offsets_kernel<<<(unsigned)ntiles, kScanThreads, 0, st>>>(count, nb + 1, tshift, tsum);
-  launches += 2;
+  launches++;
   if (n > 0) {
     cell_scatter_kernel<<<ceil_div(n, 256), 256, 0, st>>>(n, b.keys[1], b.vals[1], b.rec, b.cell_start, bm,
                                                           b.keys[0], b.vals[0], b.tkeys, b.tmp, b.rec_sorted);
