@@ -1106,6 +1106,13 @@ int launch_conv_inverse(const FftPlan3 &F, const Geom &g, const Influence &inf, 
   return k + inv_yz(F, cplx, real, partials, nb, g.cell, raw, ev, st);
 }
 
+int launch_conv_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                       const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st) {
+  int nb;
+  const int k = x_pass<XM_CONV_INV>(F, g, inf, iB0, iB1, iB2, cplx, partials, nb, st);
+  return k + launch_finish(partials, nb, g.cell, raw, nullptr, st);
+}
+
 int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st) {
   int nb;

@@ -624,12 +624,16 @@ double de1(void *p, double vir[6]) {
     printf("Error: No convolution kernel has been set.\n");
     return 0.0;
   }
-  int k = launch_conv_inverse(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_real,
-                              h->d_partials, h->d_red, h->d_ev, h->stream);
-  if (!launched(h, k, "de1 kernels")) return 0.0;
+  // The energy and virial are read as soon as the x pass has summed them; the
+  // inverse y/z passes that make the potential grid for de2/potl run on in
+  // stream order while this returns (they overlap the caller's next copies).
+  int k = launch_conv_energy(h->fft, h->geom, h->inf, h->d_iB[0], h->d_iB[1], h->d_iB[2], h->d_cplx, h->d_partials,
+                             h->d_red, h->stream);
   if (!CK(h, cudaMemcpyAsync(h->h_red, h->d_red, sizeof(double) * kRedWords, cudaMemcpyDeviceToHost, h->stream)) ||
-      !sync(h))
+      !CK(h, cudaEventRecord(h->ev_in, h->stream)))
     return 0.0;
+  k += inv_yz(h->fft, h->d_cplx, h->d_real, nullptr, 0, h->d_cell, nullptr, nullptr, h->stream);
+  if (!launched(h, k, "de1 kernels") || !CK(h, cudaEventSynchronize(h->ev_in))) return 0.0;
   const double *r = h->h_red;
   const double fac = h->hcell.iV * h->hcell.iV;
   vir[0] = (r[1] + r[0]) * fac;

@@ -78,6 +78,11 @@ int launch_fft_forward(const FftPlan3 &F, const Geom &g, const float *real, floa
 int launch_conv_inverse(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0,
                         const double *iB1, const double *iB2, float2 *cplx, float *real, double *partials,
                         double *raw, double *ev, cudaStream_t st);
+// de1's first half: x pass with the convolution, and the energy/virial sums
+// in raw (the same sums, in the same order, as launch_conv_inverse forms);
+// the caller enqueues inv_yz (without partials) afterwards.
+int launch_conv_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
+                       const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st);
 // en path: energy/virial sums of S (raw), same order as launch_conv_inverse.
 int launch_energy(const FftPlan3 &F, const Geom &g, const Influence &inf, const double *iB0, const double *iB1,
                   const double *iB2, float2 *cplx, double *partials, double *raw, cudaStream_t st);
