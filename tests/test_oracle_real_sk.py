@@ -1,7 +1,9 @@
 """CPU pins of the oracle's real-space term and radial binning, the checkers
 of the device's sfac_real_space and sfac_sk_radial: gradient and virial
 against central finite differences, the full Ewald energy of rock salt
-against its Madelung constant, and the binning against a direct loop."""
+against its Madelung constant, and the binning against a direct loop and
+against the reference's own plot.py (fixture tests/golden/plot_radial_ref.npz,
+made by tests/golden/make_plot_golden.py)."""
 import math
 
 import numpy as np
@@ -115,3 +117,32 @@ def test_sk_radial_matches_direct_loop():
                     wc[b] += 1
     np.testing.assert_array_equal(counts, wc)
     np.testing.assert_allclose(sums, ws, rtol=1e-13, atol=0)
+
+
+def test_sk_radial_matches_reference_plot_py():
+    """Per-bin sums of the reference's plot.py (plot.py:9-32), run unmodified
+    on a seeded |S|^2 array that is zero on the modes where its z fold and
+    overflow bin differ from the oracle's binning (fixture and generator in
+    tests/golden/)."""
+    import os
+    import sys
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    try:
+        import make_plot_golden as G
+    finally:
+        sys.path.remove(here)
+    z = np.load(os.path.join(here, "plot_radial_ref.npz"))
+    K, L, nbins, kmax = tuple(int(k) for k in z["K"]), float(z["L"]), int(z["nbins"]), float(z["kmax"])
+    f, kmax_gen = G.seeded_array(K, int(z["seed"]), L)
+    assert kmax_gen == kmax
+    sums, counts = O.sk_radial(np.array([L, L, L, 0, 0, 0]), K, f, nbins, kmax)
+    bins, ref = z["bins"], z["sums"]
+    inside = bins < nbins  # plot.py also prints its overflow bin (|k| >= kmax: zero here)
+    assert np.all(ref[~inside] == 0.0)
+    np.testing.assert_allclose(sums[bins[inside]], ref[inside], rtol=1e-12, atol=0)
+    rest = np.ones(nbins, bool)
+    rest[bins[inside]] = False
+    rest[0] = False  # plot.py does not print bin 0 (the k = 0 mode)
+    assert not np.any(sums[rest])
