@@ -186,8 +186,8 @@ def algorithmic_bytes(n, K):
 # profiles/dram_per_kernel_water.md.  None: not captured for the current
 # kernels.
 NCU_TRAFFIC = {
-    "water": {"cell_sort": 7.48e6, "spread": None, "fft_forward": 7.30e6, "convolution": 29.00e6,
-              "fft_inverse": 7.38e6, "gather": None},
+    "water": {"cell_sort": 7.48e6, "spread": 2.33e6, "fft_forward": 7.30e6, "convolution": 28.99e6,
+              "fft_inverse": 7.38e6, "gather": 6.70e6},
     "triclinic": {"cell_sort": 119.30e6, "spread": 46.51e6, "fft_forward": 163.58e6, "convolution": 162.71e6,
                   "fft_inverse": 165.67e6, "gather": 160.72e6},
 }
