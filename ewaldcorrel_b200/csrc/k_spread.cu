@@ -74,8 +74,8 @@ template <int P>
 struct SpStage {
   using C = SpCfg<P>;
   f2r zp[32][C::ZL];   // (wz[t], wz[t]), t < P: weight of z = rz + t
-  __align__(16) f2r wxl[32][6];   // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 6 pairs)
-  __align__(16) float wyl[32][12]; // y weights of rows 0..7 (padded to 12)
+  __align__(16) f2r wxl[32][5];  // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 5 pairs)
+  __align__(16) float wyl[32][9]; // y weights of rows 0..7 (padded to 9: the staging stores spread over the banks)
   int cnt[64];         // atoms per window case in the chunk, then the case starts
 };
 constexpr int kRowMap = 512;
@@ -310,10 +310,12 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
         float4 *zx = reinterpret_cast<float4 *>(&st.wxl[0][0]);
         float4 *zy = reinterpret_cast<float4 *>(&st.wyl[0][0]);
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        constexpr int NX = sizeof(st.wxl) / 16, NY = sizeof(st.wyl) / 16;
+        static_assert(sizeof(st.wxl) % 16 == 0 && sizeof(st.wyl) % 16 == 0, "whole 16-byte stores");
 #pragma unroll
         for (int v = 0; v < 3; v++) {
-          zx[v * 32 + lane] = z4;
-          zy[v * 32 + lane] = z4;
+          if (v * 32 + lane < NX) zx[v * 32 + lane] = z4;
+          if (v * 32 + lane < NY) zy[v * 32 + lane] = z4;
         }
       }
       __syncwarp();
