@@ -8,8 +8,12 @@
 //
 // Blocking: a warp owns an 8 x 8 x 16 brick of grid points in registers.
 // Lane (lx, ly) holds the two neighbouring columns x = 2 lx, 2 lx + 1 at
-// y = ly, 16 z points each, as 16 packed FP32 pairs, so that one packed FMA
-// (fma.rn.f32x2) adds an atom's z tap to both columns.  The brick is 16
+// y = ly, 16 z points each, as packed FP32 pairs along z (z = 2j, 2j + 1),
+// so that one packed FMA (fma.rn.f32x2) adds an atom's weight times two
+// consecutive z taps to one column (pairs along z rather than across the two
+// columns: the taps then need no duplication, 2 instead of 3 shared loads
+// per atom and brick at order 6; the same products in the same order, so the
+// same bits).  The brick is 16
 // deep rather than 32 so that the kernel fits in 64 registers: 8 CTAs of 4
 // warps per SM hide the shared-memory latency of the walk better than 5 at
 // 96 registers outweigh the longer z halo.  The atoms of the brick's halo
@@ -26,7 +30,7 @@
 // folded into x) once and stores what the lanes will read: the weights of
 // the brick's 8 x columns (as the 4 pairs the lanes hold) and 8 y rows,
 // written straight to their columns of the row after zeroing it, and the z
-// taps as duplicated pairs ready for the packed FMA.  The walk goes window
+// taps as consecutive pairs ready for the packed FMA.  The walk goes window
 // case by window case in a compile-time unrolled chain, each case a plain
 // loop over its contiguous rows: per atom, the lane's x pair and y weight,
 // two multiplies, the z taps and p packed FMAs into fixed registers -- no
@@ -66,14 +70,17 @@ struct SpCfg {
   // halo cell rows of a brick: cells [x0 - H, x0 + TX - 2 + H] (RX of them)
   static constexpr int RX = SP_TX + P - 1, RY = SP_TY + P - 1, NR = RX * RY;
   static constexpr int NC = SP_TZ + P - 1;  // window cases: first z tap rz in [1 - P, TZ - 1]
-  static constexpr int ZL = (P + 1) / 2 * 2;  // z pairs per atom (even: rows stay 16-byte aligned)
+  // z taps as consecutive pairs (z, z + 1) from the even z at or below the first
+  // tap: P + 2 values, ZQ pairs, rows rounded to whole 16-byte loads (ZQE pairs)
+  static constexpr int ZQ = P / 2 + 1;
+  static constexpr int ZQE = (ZQ + 1) / 2 * 2;
 };
 
 // Shared memory of one warp.
 template <int P>
 struct SpStage {
   using C = SpCfg<P>;
-  f2r zp[32][C::ZL];   // (wz[t], wz[t]), t < P: weight of z = rz + t
+  f2r zq[32][C::ZQE];  // (w(zs + 2m), w(zs + 2m + 1)): z taps from the even zs <= rz, zero off the stencil
   __align__(16) f2r wxl[32][5];  // x weights of columns (2 lx, 2 lx + 1), lx = 0..3 (row padded to 5 pairs)
   __align__(16) float wyl[32][9]; // y weights of rows 0..7 (padded to 9: the staging stores spread over the banks)
   int cnt[64];         // atoms per window case in the chunk, then the case starts
@@ -96,14 +103,23 @@ constexpr size_t sp_smem_bytes() {
   return SP_WARPS * (sp_stage_bytes<P, NS>() + sizeof(SpGroup<P>));
 }
 
-// acc[z] += wxy * zp[t] for the taps t whose z = C - (P - 1) + t lies in the
-// brick (all indices compile-time).
+// acc[c][j] += d_c * zq[m] for the pairs m whose z = zs + 2m lies in the brick
+// (zs: the even z at or below the first tap rz = C - (P - 1); all indices
+// compile-time); pairs that hold no tap of this case are skipped.
 template <int P, int C>
-__device__ __forceinline__ void sp_taps(f2r (&acc)[SP_TZ], f2r wxy, const f2r (&zp)[SpCfg<P>::ZL]) {
+__device__ __forceinline__ void sp_taps(f2r (&acc)[2][SP_TZ / 2], f2r d0, f2r d1,
+                                        const f2r (&zq)[SpCfg<P>::ZQE]) {
+  constexpr int rz = C - (P - 1);
+  constexpr int par = rz & 1;
+  constexpr int zs = rz - par;
+  constexpr int used = (P + par + 1) / 2;  // pairs holding taps
 #pragma unroll
-  for (int t = 0; t < P; t++) {
-    const int z = C - (P - 1) + t;
-    if (z >= 0 && z < SP_TZ) acc[z] = ffma2(wxy, zp[t], acc[z]);
+  for (int m = 0; m < used; m++) {
+    const int jz = zs / 2 + m;
+    if (jz >= 0 && jz < SP_TZ / 2) {
+      acc[0][jz] = ffma2(d0, zq[m], acc[0][jz]);
+      acc[1][jz] = ffma2(d1, zq[m], acc[1][jz]);
+    }
   }
 }
 
@@ -111,22 +127,23 @@ __device__ __forceinline__ void sp_taps(f2r (&acc)[SP_TZ], f2r wxy, const f2r (&
 // compile-time, so every accumulator index is fixed) adds the staged rows
 // [start[C], start[C + 1]); a case absent from the chunk costs one test.
 template <int P, int C>
-__device__ __forceinline__ void sp_walk(f2r (&acc)[SP_TZ], const SpStage<P> &st, int lx, int ly, int k) {
+__device__ __forceinline__ void sp_walk(f2r (&acc)[2][SP_TZ / 2], const SpStage<P> &st, int lx, int ly, int k) {
   if constexpr (C < SpCfg<P>::NC) {
     const int e = st.cnt[C + 1];
 #pragma unroll 1
     for (; k < e; k++) {
       const float2 xp = *reinterpret_cast<const float2 *>(&st.wxl[k][lx]);
       const float wy = st.wyl[k][ly];
-      const f2r wxy = pack2(xp.x * wy, xp.y * wy);
-      f2r zp[SpCfg<P>::ZL];
+      const float w0 = xp.x * wy, w1 = xp.y * wy;
+      const f2r d0 = pack2(w0, w0), d1 = pack2(w1, w1);
+      f2r zq[SpCfg<P>::ZQE];
 #pragma unroll
-      for (int v = 0; v < SpCfg<P>::ZL / 2; v++) {
-        const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zp[k][2 * v]);
-        zp[2 * v] = q.x;
-        zp[2 * v + 1] = q.y;
+      for (int v = 0; v < SpCfg<P>::ZQE / 2; v++) {
+        const ulonglong2 q = *reinterpret_cast<const ulonglong2 *>(&st.zq[k][2 * v]);
+        zq[2 * v] = q.x;
+        zq[2 * v + 1] = q.y;
       }
-      sp_taps<P, C>(acc, wxy, zp);
+      sp_taps<P, C>(acc, d0, d1, zq);
     }
     sp_walk<P, C + 1>(acc, st, lx, ly, k);
   }
@@ -193,9 +210,9 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
   const bool nearx = K0 >= RX, neary = K1 >= RY;
 
 
-  f2r acc[SP_TZ];
+  f2r acc[2][SP_TZ / 2];  // column 2 lx + c at z = 2j, 2j + 1
 #pragma unroll
-  for (int z = 0; z < SP_TZ; z++) acc[z] = 0ull;
+  for (int j = 0; j < SP_TZ / 2; j++) acc[0][j] = acc[1][j] = 0ull;
 
   // extended z cells whose stencils reach [z0, z0 + TZ): [z0 - H, z0 + TZ + H - 2],
   // walked in pieces that do not cross the periodic boundary
@@ -327,7 +344,6 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
         float *wxr = reinterpret_cast<float *>(&st.wxl[row][0]);
         float *wyr = &st.wyl[row][0];
         const int cx = hr / RY - (P - 1), cy = hr % RY - (P - 1);
-        static_assert(SpCfg<P>::ZL == P, "even orders: the z taps fill whole 16-byte pairs");
         float zt[P];
 #pragma unroll
         for (int i = 0; i < P; i++) {
@@ -338,10 +354,19 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
           if ((unsigned)(cy + i) < 8u) wyr[cy + i] = wy;
           zt[i] = wz;
         }
+        // pair m holds taps 2m - par and 2m + 1 - par (par: parity of the first tap's z)
+        const int par = (mycase - (P - 1)) & 1;
+        float zv[2 * SpCfg<P>::ZQE];
 #pragma unroll
-        for (int v = 0; v < SpCfg<P>::ZL / 2; v++)
-          *reinterpret_cast<ulonglong2 *>(&st.zp[row][2 * v]) =
-              make_ulonglong2(pack2(zt[2 * v], zt[2 * v]), pack2(zt[2 * v + 1], zt[2 * v + 1]));
+        for (int q = 0; q < 2 * SpCfg<P>::ZQE; q++) {
+          const float a = (q < P) ? zt[q] : 0.f;                      // par 0: tap q
+          const float b = (q >= 1 && q - 1 < P) ? zt[q - 1] : 0.f;   // par 1: tap q - 1
+          zv[q] = par ? b : a;
+        }
+#pragma unroll
+        for (int v = 0; v < SpCfg<P>::ZQE / 2; v++)
+          *reinterpret_cast<ulonglong2 *>(&st.zq[row][2 * v]) =
+              make_ulonglong2(pack2(zv[4 * v], zv[4 * v + 1]), pack2(zv[4 * v + 2], zv[4 * v + 3]));
       }
       __syncwarp();
       sp_walk<P, 0>(acc, st, lx, ly, 0);
@@ -360,22 +385,14 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
       if (!SPME_IN(((long)gx * K1 + gy) * K2 + min(z0 + SP_TZ, K2) - 1, (long)K0 * K1 * K2, CK_SPREAD_GRID)) continue;
       if ((K2 & 3) == 0 && z0 + SP_TZ <= K2) {
 #pragma unroll
-        for (int z = 0; z < SP_TZ; z += 4) {
-          float v[4];
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            float lo, hi;
-            unpack2(acc[z + q], lo, hi);
-            v[q] = c ? hi : lo;
-          }
-          *reinterpret_cast<float4 *>(col + z) = make_float4(v[0], v[1], v[2], v[3]);
-        }
+        for (int z = 0; z < SP_TZ; z += 4)  // a pair holds (z, z + 1), low word first: the grid's own order
+          *reinterpret_cast<ulonglong2 *>(col + z) = make_ulonglong2(acc[c][z / 2], acc[c][z / 2 + 1]);
       } else {
 #pragma unroll
         for (int z = 0; z < SP_TZ; z++) {
           float lo, hi;
-          unpack2(acc[z], lo, hi);
-          if (z0 + z < K2) col[z] = c ? hi : lo;
+          unpack2(acc[c][z / 2], lo, hi);
+          if (z0 + z < K2) col[z] = (z & 1) ? hi : lo;
         }
       }
     }
@@ -386,11 +403,14 @@ __global__ void __launch_bounds__(SP_WARPS * 32, SP_MIN_CTAS) spread_kernel(SpAr
     group_sync<NS>(group);
     float *part = reinterpret_cast<float *>(&st);  // [k * SP_TZ + z][33]: column 2 lx + k of lane
 #pragma unroll
-    for (int z = 0; z < SP_TZ; z++) {
-      float v0, v1;
-      unpack2(acc[z], v0, v1);
-      part[z * 33 + lane] = v0;
-      part[(SP_TZ + z) * 33 + lane] = v1;
+    for (int j = 0; j < SP_TZ / 2; j++) {
+      float a0, a1, b0, b1;
+      unpack2(acc[0][j], a0, a1);  // column 2 lx at z = 2j, 2j + 1
+      unpack2(acc[1][j], b0, b1);  // column 2 lx + 1
+      part[(2 * j) * 33 + lane] = a0;
+      part[(2 * j + 1) * 33 + lane] = a1;
+      part[(SP_TZ + 2 * j) * 33 + lane] = b0;
+      part[(SP_TZ + 2 * j + 1) * 33 + lane] = b1;
     }
     group_sync<NS>(group);
     const float *gpart = reinterpret_cast<const float *>(sp_smem + (size_t)group * NS * sp_stage_bytes<P, NS>());
