@@ -188,7 +188,7 @@ def algorithmic_bytes(n, K):
 NCU_TRAFFIC = {
     "water": {"cell_sort": 7.48e6, "spread": 2.33e6, "fft_forward": 7.30e6, "convolution": 28.99e6,
               "fft_inverse": 7.38e6, "gather": 6.70e6},
-    "triclinic": {"cell_sort": 119.30e6, "spread": 46.51e6, "fft_forward": 163.58e6, "convolution": 162.71e6,
+    "triclinic": {"cell_sort": 119.30e6, "spread": 44.54e6, "fft_forward": 163.58e6, "convolution": 162.71e6,
                   "fft_inverse": 165.67e6, "gather": 160.72e6},
 }
 # Kernels of each stage (the roofline is reported for the longest stage that
