@@ -10,18 +10,18 @@
 // Lane (lx, ly) holds the two neighbouring columns x = 2 lx, 2 lx + 1 at
 // y = ly, 16 z points each, as packed FP32 pairs along z (z = 2j, 2j + 1),
 // so that one packed FMA (fma.rn.f32x2) adds an atom's weight times two
-// consecutive z taps to one column (pairs along z rather than across the two
-// columns: the taps then need no duplication, 2 instead of 3 shared loads
-// per atom and brick at order 6; the same products in the same order, so the
-// same bits).  The brick is 16
-// deep rather than 32 so that the kernel fits in 64 registers: 8 CTAs of 4
-// warps per SM hide the shared-memory latency of the walk better than 5 at
-// 96 registers outweigh the longer z halo.  The atoms of the brick's halo
-// (the cells whose stencils reach it) are the sorted atoms of (x, y) cell
-// rows, found through the bucket offsets of the cell sort (runs of 32 z
-// cells per row); a brick's halo starts H = p/2 cells before a bucket
-// boundary (even bricks) or ends H - 1 cells after one (odd bricks), where
-// the sort's per-bucket tail/head counts give the cut without a search.
+// consecutive z taps to one column.  Pairs along z rather than across the
+// two columns: the taps then need no duplication (2 instead of 3 shared
+// loads per atom and brick at order 6), with the same products in the same
+// order, so the same bits.  The brick is 16 deep rather than 32 so that the
+// kernel fits in 64 registers: 8 CTAs of 4 warps per SM hide the shared-memory
+// latency of the walk better than 5 at 96 registers outweigh the longer z
+// halo.  The atoms of the brick's halo (the cells whose stencils reach it)
+// are the sorted atoms of (x, y) cell rows, found through the bucket offsets
+// of the cell sort (runs of 32 z cells per row); a brick's halo starts H = p/2
+// cells before a bucket boundary (even bricks) or ends H - 1 cells after one
+// (odd bricks), where the sort's per-bucket tail/head counts give the cut
+// without a search.
 //
 // The atoms are staged 32 at a time, one per lane, at the row given by a
 // counting sort of the chunk on its window case (the place of the atom's z
@@ -29,14 +29,14 @@
 // evaluates the order-p B-spline taps of the three fractions (the charge
 // folded into x) once and stores what the lanes will read: the weights of
 // the brick's 8 x columns (as the 4 pairs the lanes hold) and 8 y rows,
-// written straight to their columns of the row after zeroing it, and the z
-// taps as consecutive pairs ready for the packed FMA.  The walk goes window
-// case by window case in a compile-time unrolled chain, each case a plain
-// loop over its contiguous rows: per atom, the lane's x pair and y weight,
-// two multiplies, the z taps and p packed FMAs into fixed registers -- no
-// indirect jump, no divergent branch.  Small grids split one brick's atoms
-// over 2 or 4 warps (equal contiguous shares, summed in warp order through
-// shared memory: still a fixed order).
+// written straight to their columns of rows the warp has zeroed, and the z
+// taps as consecutive pairs from the even z at or below the first tap.  The
+// walk goes window case by window case in a compile-time unrolled chain,
+// each case a plain loop over its contiguous rows: per atom, the lane's x
+// pair and y weight, two multiplies, the z pairs and two packed FMAs per
+// pair into fixed registers -- no indirect jump, no divergent branch.  Small
+// grids split one brick's atoms over 2 or 4 warps (equal contiguous shares,
+// summed in warp order through shared memory: still a fixed order).
 #include "spme_kernels.hpp"
 
 namespace spme {
